@@ -1,0 +1,258 @@
+"""ctypes view of the C ABI in include/bdsim_cuda.h and the parameter packer.
+
+`pack_batch` turns per-chain (PhysParams, SimParams) into the bdcu_phys /
+bdcu_sim record arrays and the shared double arena the ABI takes.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import PhysParams, SimParams
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+c_int64_p = ctypes.POINTER(ctypes.c_int64)
+
+# status bits (bdsim_cuda.h)
+ST_NONCONVERGED = 1
+ST_NOT_PD = 2
+ST_CHEB_FALLBACK = 4
+ST_RTSAFE_FAIL = 8
+ST_NONFINITE = 16
+ST_BAD_PARAM = 32
+ST_FATAL_MASK = ST_NOT_PD | ST_RTSAFE_FAIL | ST_NONFINITE | ST_BAD_PARAM
+
+FORM_PLAIN_FP64 = 0
+FORM_MIXED_FP32 = 1
+CACHE_RESET_PER_CALL = 0
+CACHE_PERSIST = 1
+
+STATUS_NAMES = {
+    ST_NONCONVERGED: "corrector did not converge",
+    ST_NOT_PD: "cholesky_lower: matrix is not positive definite",
+    ST_CHEB_FALLBACK: "Chebyshev fluctuation-dissipation check failed (Cholesky fallback)",
+    ST_RTSAFE_FAIL: "rtsafe failed (root not bracketed or max iterations)",
+    ST_NONFINITE: "bead positions became non-finite",
+    ST_BAD_PARAM: "invalid parameter (WLCbounded sigma > 1 or ExactSqrt)",
+}
+
+
+class BdcuPhys(ctypes.Structure):
+    _fields_ = [
+        ("n_beads", ctypes.c_int32),
+        ("spring_type", ctypes.c_int32),
+        ("sqrtb", ctypes.c_double),
+        ("natural_length", ctypes.c_double),
+        ("ev_type", ctypes.c_int32),
+        ("contour_dist_for_ev", ctypes.c_int32),
+        ("zstar", ctypes.c_double),
+        ("dstar", ctypes.c_double),
+        ("min_cutoff", ctypes.c_double),
+        ("max_cutoff", ctypes.c_double),
+        ("phi_offset", ctypes.c_int64),
+        ("bend_type", ctypes.c_int32),
+        ("equilibration", ctypes.c_int32),
+        ("bend_stiffness", ctypes.c_double),
+        ("hstar", ctypes.c_double),
+        ("hi_method", ctypes.c_int32),
+        ("flow_n_times", ctypes.c_int32),
+        ("ncheb_multiplier", ctypes.c_double),
+        ("fd_err_max", ctypes.c_double),
+        ("flow_kappa", ctypes.c_double * 9),
+        ("flow_offset", ctypes.c_int64),
+        ("ext_n_entries", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+        ("ext_offset", ctypes.c_int64),
+    ]
+
+
+class BdcuSim(ctypes.Structure):
+    _fields_ = [
+        ("time_start", ctypes.c_double),
+        ("time_end", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("implicit_loop_tol", ctypes.c_double),
+        ("update_center_of_mass", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+    ]
+
+
+class BdcuCounters(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in (
+        "steps", "dx_products", "cheb_terms", "corrector_iters",
+        "lanczos_cold", "lanczos_warm", "cheb_fallbacks", "nonconverged")]
+
+
+COUNTER_FIELDS = [f[0] for f in BdcuCounters._fields_]
+
+
+class _Arena:
+    def __init__(self):
+        self.chunks = []
+        self.size = 0
+        self._memo = {}
+
+    def add(self, values, key=None):
+        if key is not None and key in self._memo:
+            return self._memo[key]
+        arr = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        off = self.size
+        self.chunks.append(arr)
+        self.size += arr.size
+        if key is not None:
+            self._memo[key] = off
+        return off
+
+    def array(self):
+        if not self.chunks:
+            return np.zeros(1, dtype=np.float64)
+        return np.concatenate(self.chunks)
+
+
+def _fill_phys(rec: BdcuPhys, phys: PhysParams, n_beads: int, arena: _Arena):
+    rec.n_beads = int(n_beads)
+    rec.spring_type = int(phys.spring.type)
+    rec.sqrtb = float(phys.spring.sqrtb)
+    rec.natural_length = float(phys.spring.natural_length)
+    ev = phys.ev
+    rec.ev_type = int(ev.type)
+    rec.contour_dist_for_ev = int(ev.contour_dist_for_EV)
+    rec.zstar = float(ev.zstar)
+    rec.dstar = float(ev.dstar)
+    rec.min_cutoff = float(ev.min_cutoff)
+    rec.max_cutoff = float(ev.max_cutoff)
+    rec.phi_offset = -1
+    if len(ev.phi) > 0:
+        phi = np.asarray(ev.phi, dtype=np.float64).reshape(-1)
+        if phi.size != n_beads * n_beads:
+            raise ValueError(f"EVParams.phi must hold N*N={n_beads * n_beads} values, got {phi.size}")
+        rec.phi_offset = arena.add(phi, key=("phi", phi.tobytes()))
+    rec.bend_type = int(phys.bend.type)
+    rec.equilibration = int(bool(phys.equilibration))
+    rec.bend_stiffness = float(phys.bend.stiffness)
+    rec.hstar = float(phys.hstar)
+    rec.hi_method = int(phys.hi_method)
+    rec.ncheb_multiplier = float(phys.ncheb_multiplier)
+    rec.fd_err_max = float(phys.fd_err_max)
+    fl = phys.flow
+    for i, v in enumerate(np.asarray(fl._k0, dtype=np.float64).reshape(-1)):
+        rec.flow_kappa[i] = float(v)
+    if fl.is_constant():
+        rec.flow_n_times = 0
+        rec.flow_offset = 0
+    else:
+        rec.flow_n_times = len(fl._times)
+        rec.flow_offset = arena.add(np.concatenate([fl._times, fl._ks.reshape(-1)]),
+                                    key=("flow", fl._times.tobytes(), fl._ks.tobytes()))
+    ents = phys.external.entries()
+    rec.ext_n_entries = len(ents)
+    rec.ext_offset = 0
+    if ents:
+        buf = []
+        for bead, is_const, val, times, vals in ents:
+            n = len(times)
+            buf += [float(bead), 1.0 if is_const else 0.0, *val, float(n), *times]
+            for v in vals:
+                buf += list(v)
+        rec.ext_offset = arena.add(np.array(buf), key=("ext", tuple(buf)))
+
+
+def _fill_sim(rec: BdcuSim, sim: SimParams):
+    rec.time_start = float(sim.time_start)
+    rec.time_end = float(sim.time_end)
+    rec.dt = float(sim.dt)
+    rec.implicit_loop_tol = float(sim.implicit_loop_tol)
+    rec.update_center_of_mass = int(bool(sim.update_center_of_mass))
+
+
+def pack_batch(phys_list, sim_list, n_beads_list):
+    """-> (phys_array ctypes, sim_array ctypes, arena float64 ndarray)."""
+    n = len(phys_list)
+    if not (len(sim_list) == n == len(n_beads_list)):
+        raise ValueError("phys, sim and n_beads lists must have equal length")
+    arena = _Arena()
+    phys_arr = (BdcuPhys * max(n, 1))()
+    sim_arr = (BdcuSim * max(n, 1))()
+    for i in range(n):
+        _fill_phys(phys_arr[i], phys_list[i], n_beads_list[i], arena)
+        _fill_sim(sim_arr[i], sim_list[i])
+    return phys_arr, sim_arr, arena.array()
+
+
+def count_steps(sim: SimParams) -> int:
+    """Steps the reference loop `for (t = t0; t <= t1 + dt/2; t += dt)`
+    takes (src/integrator.cpp:102), replayed in double arithmetic."""
+    t, t1, dt = float(sim.time_start), float(sim.time_end), float(sim.dt)
+    if not dt > 0.0:
+        raise ValueError("dt must be positive")
+    lim = t1 + dt / 2.0
+    n = 0
+    while t <= lim:
+        n += 1
+        t += dt
+    return n
+
+
+def dptr(a) -> ctypes.c_void_p:
+    """Raw pointer of a numpy array or torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+_LIB = None
+LIB_NAME = "libbdsim_cuda.so"
+
+
+def lib_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+
+def load_library():
+    """Load the CUDA integrator library. Raises if it was not built: there is
+    no CPU fallback."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = lib_path()
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"bdsim_b200: the CUDA integrator library {path} is missing; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (or `make -C bdsim_b200/csrc`). "
+            "There is no CPU fallback.")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    lib.bdcu_version.restype = ctypes.c_char_p
+    lib.bdcu_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    lib.bdcu_destroy.argtypes = [vp]
+    lib.bdcu_set_stream.argtypes = [vp, vp]
+    lib.bdcu_last_error.argtypes = [vp]
+    lib.bdcu_last_error.restype = ctypes.c_char_p
+    lib.bdcu_set_chains.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim),
+                                    c_double_p, ctypes.c_int64]
+    lib.bdcu_count_steps.argtypes = [ctypes.POINTER(BdcuSim), c_int64_p]
+    lib.bdcu_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
+    lib.bdcu_integrate_host.argtypes = [vp, c_double_p, c_int32_p, c_int32_p,
+                                        ctypes.POINTER(BdcuCounters), ctypes.c_int]
+    lib.bdcu_total_force.argtypes = [vp, vp, vp]
+    lib.bdcu_forces.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp]
+    lib.bdcu_ran1.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]
+    for name in ("bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
+                 "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
+                 "bdcu_forces", "bdcu_ran1"):
+        getattr(lib, name).restype = ctypes.c_int
+    _LIB = lib
+    return lib
+
+
+# Symbols include/bdsim_cuda.h declares (checked by the CPU test suite).
+EXPORTED_SYMBOLS = [
+    "bdcu_version", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_last_error",
+    "bdcu_set_chains", "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host",
+    "bdcu_total_force", "bdcu_forces", "bdcu_ran1",
+]
+
+F_SPRING, F_EV, F_BEND, F_EXTERNAL = 1, 2, 4, 8

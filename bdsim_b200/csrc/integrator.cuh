@@ -1,0 +1,1067 @@
+// integrator.cuh -- the ChainIntegrator step loop as one persistent sm_100a
+// kernel: one chain per thread block, chains claimed from a device work queue,
+// chain state resident in shared memory for all steps of a call.
+//
+// FORM == BDCU_FORM_PLAIN_FP64: the reference algorithm in FP64. The dense RPY
+//   tensor D lives in shared memory (global scratch when 3N is too large);
+//   D.x is a row-sequential sum per thread, EV forces are accumulated per bead
+//   in the reference's pair order, Cholesky is right-looking with the
+//   reference's per-element subtraction order. Only block dot products
+//   (Lanczos, FD check) use a tree order.
+// FORM == BDCU_FORM_MIXED_FP32: D.x recomputed pairwise in FP32 from
+//   shared-memory bead coordinates (no stored D), FP32 excluded volume; FP64
+//   positions, connector solve, Lanczos bounds and Cholesky.
+//
+// Reference: src/integrator.cpp:61-170 of the bdsim project and the physics
+// it calls (cited per function).
+#pragma once
+
+#include <stdint.h>
+
+#include "bdcu_internal.h"
+#include "device_physics.cuh"
+
+namespace bdcu {
+
+constexpr int kSlots = 16;     // n-vectors in shared memory
+constexpr int kCoefCap = 504;  // >= kMaxCheb + 1
+
+// Block-shared control state.
+struct Ctl {
+    double com[3];
+    double lmin, lmax, x0Dx0, fd_err, incr, rmin, rmax, glo, ghi, nv, bval;
+    int32_t chain, k, L, status, cache_valid, lz_steps, brk, pad;
+    int64_t cnt[8];  // bdcu_counters order
+};
+enum { C_STEPS = 0, C_DX, C_CHEB, C_CORR, C_LZCOLD, C_LZWARM, C_FALLBACK, C_NONCONV };
+
+struct SmemLayout {
+    int64_t ctl, chain, red, alpha, beta, ymin, ymax, coef, sqx, slots, V, D, f32, total;  // in doubles
+};
+
+__host__ __device__ inline int64_t round_up8(int64_t x) { return (x + 7) / 8 * 8; }
+
+// Shared-memory layout (in doubles) for a launch whose largest chain has
+// 3N = n_max. Host and device compute it with the same function.
+__host__ __device__ inline SmemLayout smem_layout(int n_max, int d_in_smem, int v_cap, int mixed) {
+    SmemLayout s;
+    int64_t o = 0;
+    s.ctl = o;   o += round_up8((int64_t)(sizeof(Ctl) + 7) / 8);
+    s.chain = o; o += round_up8((int64_t)(sizeof(DevChain) + 7) / 8);
+    s.red = o;   o += 32;
+    s.alpha = o; o += 32;
+    s.beta = o;  o += 32;
+    s.ymin = o;  o += 32;
+    s.ymax = o;  o += 32;
+    s.coef = o;  o += kCoefCap;
+    s.sqx = o;   o += kCoefCap;
+    const int64_t nv = round_up8(n_max);
+    s.slots = o; o += (int64_t)kSlots * nv;
+    s.V = o;     o += (int64_t)v_cap * nv;
+    s.D = o;     if (d_in_smem) o += (int64_t)n_max * n_max;
+    s.f32 = o;   if (mixed) o += 2 * nv;  // float4 bead coordinates + float4 staged vector (N <= n/3 each)
+    s.total = o;
+    return s;
+}
+
+// Global scratch per thread block (doubles): dense D when it is not in shared
+// memory (plain form), the Cholesky factor, and the cold Lanczos basis.
+struct ScratchLayout {
+    int64_t D, Lt, V, total;
+};
+__host__ __device__ inline ScratchLayout scratch_layout(int n_max, int d_in_smem, int v_cap, int need_chol,
+                                                        int mixed, int need_d, int need_lz) {
+    ScratchLayout s;
+    int64_t o = 0;
+    const int64_t nn = (int64_t)n_max * n_max;
+    s.D = o;  if (!mixed && need_d && !d_in_smem) o += nn;
+    s.Lt = o; if (need_chol) o += nn;
+    s.V = o;  if (need_lz && v_cap < kLanczosCold) o += (int64_t)kLanczosCold * round_up8(n_max);
+    s.total = o;
+    return s;
+}
+
+// ---------------------------------------------------------------- helpers
+
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Dot product over the block, same value returned to every thread. Order: a
+// fixed tree (not the reference's sequential order; differences are at the
+// last bit of each sum).
+static __device__ double block_dot(const double* a, const double* b, int n, double* red) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += a[i] * b[i];
+    s = warp_allsum(s);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double t = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int w = 0; w < nw; ++w) t += red[w];
+    return t;
+}
+
+// y = D x, one row per thread, summed over j in order (matvec,
+// src/linalg.cpp:81-89). D is exactly symmetric (rpy_diffusion_matrix writes
+// both halves from one value), so row i is read as column i for coalescing.
+__device__ __forceinline__ void matvec_dense(const double* __restrict__ D, int ld, const double* __restrict__ x,
+                                             double* __restrict__ y, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s = 0.0;
+        const double* col = D + i;
+#pragma unroll 8
+        for (int j = 0; j < n; ++j) s += col[(int64_t)j * ld] * x[j];
+        y[i] = s;
+    }
+}
+
+// sturm_count (src/hydrodynamics.cpp:91-104)
+__device__ __forceinline__ int sturm_count(const double* a, const double* b, int m, double x) {
+    int count = 0;
+    double d = a[0] - x;
+    if (d < 0.0) ++count;
+    for (int i = 1; i < m; ++i) {
+        if (d == 0.0) d = 1.0e-300;
+        d = (a[i] - x) - b[i - 1] * b[i - 1] / d;
+        if (d < 0.0) ++count;
+    }
+    return count;
+}
+
+// The 100-step bisection of lanczos_extremes (src/hydrodynamics.cpp:251-260),
+//   mid = 0.5*(lo+hi); if (sturm(mid) >= target) hi = mid; else lo = mid;
+// evaluated five levels at a time by one warp: lane l owns node l of a
+// depth-5 decision tree, replays the midpoints on its path with the same
+// arithmetic, and evaluates its own Sturm count; the warp then walks the
+// resolved path. A round that leaves (lo, hi) unchanged has reached the fixed
+// point of the iteration, so the remaining rounds are skipped. The result is
+// the sequential algorithm's, bit for bit.
+static __device__ void warp_bisect(const double* al, const double* bb, int k, int target, double& lo, double& hi) {
+    const int lane = threadIdx.x & 31;
+    const int lvl = 31 - __clz(lane + 1);
+    const int p = lane + 1 - (1 << lvl);
+    for (int it = 0; it < 100; it += 5) {
+        int dec = 0;
+        if (lane < 31) {
+            double a = lo, b = hi;
+            for (int l = 0; l < lvl; ++l) {
+                const int bit = (p >> (lvl - 1 - l)) & 1;
+                const double m = 0.5 * (a + b);
+                if (bit == 0) b = m; else a = m;
+            }
+            const double mid = 0.5 * (a + b);
+            dec = (sturm_count(al, bb, k, mid) >= target) ? 0 : 1;
+        }
+        int node = 0;
+        double na = lo, nb = hi;
+#pragma unroll
+        for (int l = 0; l < 5; ++l) {
+            const int d = __shfl_sync(0xffffffffu, dec, node);
+            const double m = 0.5 * (na + nb);
+            if (d == 0) nb = m; else na = m;
+            node = 2 * node + 1 + d;
+        }
+        const bool same = (na == lo && nb == hi);
+        lo = na;
+        hi = nb;
+        if (same) break;
+    }
+}
+
+// tridiag_eigenvector (src/hydrodynamics.cpp:106-136), one thread.
+static __device__ void tridiag_eigenvector(const double* a, const double* b, int m, double lambda, double* y) {
+    const double scale = dmax_(fabs(lambda), 1.0);
+    const double shift = lambda - 1.0e-7 * scale;
+    double c[kLanczosCold], d[kLanczosCold];
+    for (int i = 0; i < m; ++i) y[i] = 1.0 / sqrt((double)m);
+    for (int it = 0; it < 2; ++it) {
+        double beta0 = a[0] - shift;
+        if (fabs(beta0) < 1.0e-300) beta0 = 1.0e-300;
+        c[0] = (m > 1 ? b[0] / beta0 : 0.0);
+        d[0] = y[0] / beta0;
+        for (int i = 1; i < m; ++i) {
+            double beta = (a[i] - shift) - b[i - 1] * c[i - 1];
+            if (fabs(beta) < 1.0e-300) beta = 1.0e-300;
+            c[i] = (i < m - 1 ? b[i] / beta : 0.0);
+            d[i] = (y[i] - b[i - 1] * d[i - 1]) / beta;
+        }
+        y[m - 1] = d[m - 1];
+        for (int i = m - 2; i >= 0; --i) y[i] = d[i] - c[i] * y[i + 1];
+        double nrm = 0.0;
+        for (int i = 0; i < m; ++i) nrm += y[i] * y[i];
+        nrm = sqrt(nrm);
+        if (!(nrm > 0.0) || !isfinite(nrm)) {
+            for (int i = 0; i < m; ++i) y[i] = 1.0 / sqrt((double)m);
+            return;
+        }
+        for (int i = 0; i < m; ++i) y[i] /= nrm;
+    }
+}
+
+// --------------------------------------------------------- the block state
+
+template <int FORM>
+struct Block {
+    static constexpr bool kMixed = (FORM == BDCU_FORM_MIXED_FP32);
+    const RunArgs& a;
+    Ctl& ctl;
+    const DevChain& ch;
+    double* red;
+    double* alpha;
+    double* beta;
+    double* ymin;
+    double* ymax;
+    double* coef;
+    double* sqx;
+    double* slot[kSlots];
+    double* Vs;        // shared Lanczos basis (v_cap vectors)
+    double* Vg;        // global Lanczos basis (kLanczosCold vectors)
+    double* D;         // plain: dense D (shared or global)
+    int ldd;
+    double* Lt;        // transposed Cholesky factor, global scratch (ld = n)
+    float4* pos32;     // mixed: FP32 bead coordinates
+    float4* vec32;     // mixed: FP32 staged vector
+    int ldv;           // stride of Lanczos basis vectors
+    int N, n;
+    bool hi;
+
+    __device__ Block(const RunArgs& a_, Ctl& c_, const DevChain& ch_) : a(a_), ctl(c_), ch(ch_) {}
+
+    __device__ __forceinline__ void sync() { __syncthreads(); }
+
+    __device__ __forceinline__ void count(int which, int64_t v) {
+        if (threadIdx.x == 0) ctl.cnt[which] += v;
+    }
+
+    // ---- D.x (Diffusion::apply, src/mobility.cpp:53-56) -----------------
+    // Caller syncs before (x ready) and after (y ready). Identity => copy.
+    __device__ void apply_D(const double* x, double* y) {
+        if (!hi) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = x[i];
+            return;
+        }
+        count(C_DX, 1);
+        if constexpr (!kMixed) {
+            matvec_dense(D, ldd, x, y, n);
+        } else {
+            apply_D_pairwise(x, y);
+        }
+    }
+
+    // Matrix-free FP32 D.x: y_b = x_b + sum_{j != b} (om1 x_j + om2 (d.x_j) d),
+    // d = R_j - R_b, with omega from the RPY formula (src/hydrodynamics.cpp:77-105).
+    __device__ void apply_D_pairwise(const double* x, double* y) {
+        for (int b = threadIdx.x; b < N; b += blockDim.x)
+            vec32[b] = make_float4((float)x[3 * b], (float)x[3 * b + 1], (float)x[3 * b + 2], 0.f);
+        __syncthreads();
+        const float hs = (float)ch.hstar;
+        const float RPI = 1.7724538509055160f, TRPI = 2.f * RPI, TPI = 6.283185307179586f;
+        const float C1 = TPI / 3.f, C3 = 0.75f / RPI * 0.375f, C7 = 0.09375f / RPI, RPI3by4 = RPI * 0.75f;
+        for (int b = threadIdx.x; b < N; b += blockDim.x) {
+            const float4 rb = pos32[b];
+            const float4 xb = vec32[b];
+            float a0 = xb.x, a1 = xb.y, a2 = xb.z;
+            for (int j = 0; j < N; ++j) {
+                if (j == b) continue;
+                const float4 rj = pos32[j];
+                const float4 xj = vec32[j];
+                const float d0 = rj.x - rb.x, d1 = rj.y - rb.y, d2 = rj.z - rb.z;
+                float sq = d0 * d0 + d1 * d1 + d2 * d2;
+                sq = fmaxf(sq, 1e-12f);
+                const float rinv = rsqrtf(sq);
+                const float rs = sq * rinv;
+                const float hsbyrs = hs * rinv, rsbyhs = rs / hs;
+                const float h2 = hsbyrs * hsbyrs;
+                float om1, om2;
+                if (rsbyhs >= TRPI) {
+                    om1 = RPI3by4 * hsbyrs * (1.f + C1 * h2);
+                    om2 = RPI3by4 * hsbyrs * rinv * rinv * (1.f - TPI * h2);
+                } else {
+                    om1 = 1.f - C3 * rsbyhs;
+                    om2 = C7 * rsbyhs * rinv * rinv;
+                }
+                const float dx = om2 * (d0 * xj.x + d1 * xj.y + d2 * xj.z);
+                a0 += om1 * xj.x + dx * d0;
+                a1 += om1 * xj.y + dx * d1;
+                a2 += om1 * xj.z + dx * d2;
+            }
+            y[3 * b] = a0;
+            y[3 * b + 1] = a1;
+            y[3 * b + 2] = a2;
+        }
+    }
+
+    // ---- RPY tensor (rpy_diffusion_matrix, src/hydrodynamics.cpp:12-54) --
+    // Writes the dense D at ptr with leading dimension ld. For pair mu<nu the
+    // value of element (3mu+i, 3nu+j) and its mirror is
+    // om2*b_i*b_j + (i==j ? om1 : 0).
+    __device__ void build_rpy(const double* R, double* Dp, int ld) {
+        for (int idx = threadIdx.x; idx < 9 * N; idx += blockDim.x) {
+            const int mu = idx / 9, i = (idx % 9) / 3, j = idx % 3;
+            Dp[(int64_t)(3 * mu + i) * ld + 3 * mu + j] = (i == j) ? 1.0 : 0.0;
+        }
+        const int npairs = N * (N - 1) / 2;
+        for (int pidx = threadIdx.x; pidx < npairs; pidx += blockDim.x) {
+            int nu = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pidx)) * 0.5);
+            while (nu * (nu - 1) / 2 > pidx) --nu;
+            while ((nu + 1) * nu / 2 <= pidx) ++nu;
+            const int mu = pidx - nu * (nu - 1) / 2;
+            double b[3];
+            for (int d = 0; d < 3; ++d) b[d] = R[3 * nu + d] - R[3 * mu + d];
+            const double sq = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+            double om1, om2;
+            rpy_weights(ch.hstar, sq, om1, om2);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double val = om2 * b[i] * b[j] + (i == j ? om1 : 0.0);
+                    Dp[(int64_t)(3 * mu + i) * ld + 3 * nu + j] = val;
+                    Dp[(int64_t)(3 * nu + j) * ld + 3 * mu + i] = val;
+                }
+        }
+    }
+
+    // ---- Cholesky (cholesky_lower, src/linalg.cpp:91-107) ---------------
+    // Right-looking on Lt = L^T (Lt[k*n + i] = L(i,k)). Element (i,j) receives
+    // M(i,j) - L(i,0)L(j,0) - L(i,1)L(j,1) - ... in k order, then / L(j,j):
+    // the reference's rounding sequence. Returns false on a pivot <= 0.
+    // src: dense D at (Dp, ld) or, if src_in_lt, Lt already holds D's lower part.
+    __device__ bool cholesky(const double* Dp, int ld, bool src_in_lt) {
+        double* L = Lt;
+        if (!src_in_lt) {
+            for (int j = threadIdx.x >> 5; j < n; j += blockDim.x >> 5)
+                for (int i = j + (threadIdx.x & 31); i < n; i += 32) L[(int64_t)j * n + i] = Dp[(int64_t)i * ld + j];
+        }
+        __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            if (threadIdx.x == 0) {
+                const double s = L[(int64_t)k * n + k];
+                if (!(s > 0.0)) ctl.brk = 1; else L[(int64_t)k * n + k] = sqrt(s);
+            }
+            __syncthreads();
+            if (ctl.brk) return false;
+            const double dk = L[(int64_t)k * n + k];
+            for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) L[(int64_t)k * n + i] = L[(int64_t)k * n + i] / dk;
+            __syncthreads();
+            const double* colk = L + (int64_t)k * n;
+            for (int j = k + 1 + (threadIdx.x >> 5); j < n; j += blockDim.x >> 5) {
+                const double ljk = colk[j];
+                for (int i = j + (threadIdx.x & 31); i < n; i += 32)
+                    L[(int64_t)j * n + i] = L[(int64_t)j * n + i] - colk[i] * ljk;
+            }
+            __syncthreads();
+        }
+        return true;
+    }
+
+    // y = L x (lower_matvec, src/linalg.cpp:109-117), row sums in j order.
+    __device__ void lower_matvec(const double* x, double* y) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double s = 0.0;
+            for (int j = 0; j <= i; ++j) s += Lt[(int64_t)j * n + i] * x[j];
+            y[i] = s;
+        }
+    }
+
+    // ---- forces ---------------------------------------------------------
+
+    // Bonds (N-1 x 3) and clamped lengths of R (chain_geometry, src/config.cpp:15-25).
+    __device__ void geometry(const double* R, double* bond, double* len) {
+        for (int b = threadIdx.x; b < N - 1; b += blockDim.x) {
+            const double b0 = R[3 * b + 3] - R[3 * b], b1 = R[3 * b + 4] - R[3 * b + 1],
+                         b2 = R[3 * b + 5] - R[3 * b + 2];
+            bond[3 * b] = b0;
+            bond[3 * b + 1] = b1;
+            bond[3 * b + 2] = b2;
+            len[b] = clamped_len(b0, b1, b2);
+        }
+    }
+
+    // Spring bead forces from bonds (connector_forces + bead_forces_from_connectors,
+    // src/spring.cpp:234-254). Fc: scratch for the bond forces.
+    __device__ void spring_from_geometry(const double* bond, const double* len, double* Fc, double* F) {
+        for (int b = threadIdx.x; b < N - 1; b += blockDim.x) {
+            const double f = connector_factor(ch, len[b]);
+            Fc[3 * b] = f * bond[3 * b];
+            Fc[3 * b + 1] = f * bond[3 * b + 1];
+            Fc[3 * b + 2] = f * bond[3 * b + 2];
+        }
+        __syncthreads();
+        bead_forces(Fc, F);
+    }
+
+    __device__ void bead_forces(const double* Fc, double* F) {
+        for (int i = threadIdx.x; i < N; i += blockDim.x)
+            for (int d = 0; d < 3; ++d) {
+                double v;
+                if (i == 0) v = Fc[d];
+                else if (i == N - 1) v = (-1.0) * Fc[3 * (N - 2) + d];
+                else v = Fc[3 * i + d] - Fc[3 * (i - 1) + d];
+                F[3 * i + d] = v;
+            }
+    }
+
+    // Excluded-volume force on bead b (ExcludedVolume::force,
+    // src/excluded_volume.cpp:60-89): bead b receives -f(j,b) for j<b, then
+    // +f(b,j) for j>b, in ascending j -- the reference loop's order.
+    __device__ void ev_on_bead(const double* R, int b, double f[3]) {
+        f[0] = f[1] = f[2] = 0.0;
+        if (ch.ev_type == BDCU_EV_NONE) return;
+        const double* phi = (ch.ev_type == BDCU_EV_SDK && ch.phi_off >= 0) ? a.arena + ch.phi_off : nullptr;
+        if constexpr (!kMixed) {
+            for (int j = 0; j < N; ++j) {
+                if (j == b) continue;
+                const int mu = j < b ? j : b, nu = j < b ? b : j;
+                if ((nu - mu) < ch.cd) continue;
+                const double q0 = R[3 * nu] - R[3 * mu], q1 = R[3 * nu + 1] - R[3 * mu + 1],
+                             q2 = R[3 * nu + 2] - R[3 * mu + 2];
+                double sq = q0 * q0 + q1 * q1 + q2 * q2;
+                if (sq < 1.0e-12) sq = 1.0e-12;
+                const double r = sqrt(sq);
+                const double fac = ev_factor(ch, r, phi ? phi[mu * N + nu] : 0.0);
+                const double g0 = (-fac) * q0, g1 = (-fac) * q1, g2 = (-fac) * q2;
+                if (b == mu) {
+                    f[0] = f[0] + g0; f[1] = f[1] + g1; f[2] = f[2] + g2;
+                } else {
+                    f[0] = f[0] - g0; f[1] = f[1] - g1; f[2] = f[2] - g2;
+                }
+            }
+        } else {
+            // FP32 pair sums from the staged FP32 coordinates.
+            const float4 rb = pos32[b];
+            float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+            const float zs = (float)ch.zsbyds5, p5 = (float)ch.pt5bydssq;
+            for (int j = 0; j < N; ++j) {
+                if (j == b) continue;
+                const int mu = j < b ? j : b, nu = j < b ? b : j;
+                if ((nu - mu) < ch.cd) continue;
+                const float4 rj = pos32[j];
+                // q = R_nu - R_mu; the force on b is -fac*q if b == mu, +fac*q if b == nu
+                const float s = (b == mu) ? 1.f : -1.f;
+                const float q0 = s * (rj.x - rb.x), q1 = s * (rj.y - rb.y), q2 = s * (rj.z - rb.z);
+                float sq = fmaxf(q0 * q0 + q1 * q1 + q2 * q2, 1e-12f);
+                const float r = sqrtf(sq);
+                float fac;
+                if (ch.ev_type == BDCU_EV_GAUSS) {
+                    fac = zs * __expf(-sq * p5);
+                } else {
+                    fac = (float)ev_factor(ch, (double)r, phi ? phi[mu * N + nu] : 0.0);
+                }
+                const float g = (b == mu) ? -fac : fac;
+                f0 += g * q0;
+                f1 += g * q1;
+                f2 += g * q2;
+            }
+            f[0] = f0;
+            f[1] = f1;
+            f[2] = f2;
+        }
+    }
+
+    // Explicit force Fe = (EV + bending)(R) + external(t) (src/model.hpp:56-64,
+    // src/integrator.cpp:110-111). bond/len: geometry of R (already computed);
+    // u, cs: scratch.
+    __device__ void explicit_force(const double* R, double t, const double* bond, const double* len, double* u,
+                                   double* cs, double* out, bool with_external = true) {
+        const bool bend = (ch.bend_type != BDCU_BEND_NONE) && N > 2;
+        if (bend) {
+            for (int b = threadIdx.x; b < N - 1; b += blockDim.x)
+                for (int d = 0; d < 3; ++d) u[3 * b + d] = (1.0 / len[b]) * bond[3 * b + d];
+            __syncthreads();
+            for (int b = threadIdx.x; b < N - 2; b += blockDim.x)
+                cs[b] = u[3 * (b + 1)] * u[3 * b] + u[3 * (b + 1) + 1] * u[3 * b + 1] + u[3 * (b + 1) + 2] * u[3 * b + 2];
+            __syncthreads();
+        }
+        for (int m = threadIdx.x; m < N; m += blockDim.x) {
+            double fe[3], fb[3] = {0.0, 0.0, 0.0}, fx[3] = {0.0, 0.0, 0.0};
+            ev_on_bead(R, m, fe);
+            if (bend) bending_on_bead(ch, m, u, cs, len, fb);
+            if (!with_external) {
+                for (int d = 0; d < 3; ++d) out[3 * m + d] = fe[d] + fb[d];
+                continue;
+            }
+            if (ch.ext_n > 0) external_on_bead(ch, a.arena, m, t, fx);
+            for (int d = 0; d < 3; ++d) out[3 * m + d] = (fe[d] + fb[d]) + fx[d];
+        }
+    }
+
+    // ---- Lanczos bounds --------------------------------------------------
+
+    __device__ double* Vvec(int j, int m) { return (m <= a.v_cap ? Vs : Vg) + (int64_t)j * ldv; }
+
+    // lanczos_extremes (src/hydrodynamics.cpp:146-221). Writes alpha/beta,
+    // ctl.rmin/rmax, ctl.lz_steps, and the Ritz vectors into vmin/vmax.
+    __device__ void lanczos(int m, bool warm, const double* cache, double* w, double* vmin, double* vmax) {
+        if (n < m) m = n;
+        double* V0 = Vvec(0, m);
+        if (warm) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) V0[i] = cache[i];
+            __syncthreads();
+            double nv = sqrt(block_dot(V0, V0, n, red));
+            if (!(nv > 0.0)) {
+                for (int i = threadIdx.x; i < n; i += blockDim.x) V0[i] = a.seed_table[i];
+                nv = ch.seed_norm;
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += blockDim.x) V0[i] = V0[i] / nv;
+        } else {
+            const double nv = ch.seed_norm;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) V0[i] = a.seed_table[i] / nv;
+        }
+        __syncthreads();
+        int k = 0;
+        double b = 0.0;
+        for (int j = 0; j < m; ++j) {
+            double* v = Vvec(j, m);
+            const double* vprev = (j > 0) ? Vvec(j - 1, m) : nullptr;
+            apply_D(v, w);
+            __syncthreads();
+            const double al = block_dot(v, w, n, red);
+            if (threadIdx.x == 0) alpha[k] = al;
+            ++k;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const double vp = vprev ? vprev[i] : 0.0;
+                w[i] -= al * v[i] + b * vp;
+            }
+            __syncthreads();
+            for (int u = 0; u <= j; ++u) {
+                const double* uu = Vvec(u, m);
+                const double dd = block_dot(w, uu, n, red);
+                for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] -= dd * uu[i];
+                __syncthreads();
+            }
+            b = sqrt(block_dot(w, w, n, red));
+            if (b < 1.0e-10) break;
+            if (j + 1 < m) {
+                double* vn = Vvec(j + 1, m);
+                for (int i = threadIdx.x; i < n; i += blockDim.x) vn[i] = w[i] / b;
+            }
+            if (threadIdx.x == 0) beta[j] = b;
+            __syncthreads();
+        }
+        __syncthreads();
+        if (k == 1) {
+            if (threadIdx.x == 0) {
+                ctl.rmin = alpha[0];
+                ctl.rmax = alpha[0];
+                ctl.lz_steps = 1;
+            }
+            for (int i = threadIdx.x; i < n; i += blockDim.x) vmin[i] = vmax[i] = V0[i];
+            __syncthreads();
+            return;
+        }
+        // Gershgorin bracket (src/hydrodynamics.cpp:242-249)
+        if (threadIdx.x == 0) {
+            double lo = alpha[0], hi = alpha[0];
+            for (int i = 0; i < k; ++i) {
+                const double rad = (i > 0 ? fabs(beta[i - 1]) : 0.0) + (i < k - 1 ? fabs(beta[i]) : 0.0);
+                lo = dmin_(lo, alpha[i] - rad);
+                hi = dmax_(hi, alpha[i] + rad);
+            }
+            ctl.glo = lo;
+            ctl.ghi = hi;
+            ctl.lz_steps = k;
+        }
+        __syncthreads();
+        const int warp = threadIdx.x >> 5;
+        if (warp < 2) {
+            double lo = ctl.glo, hi = ctl.ghi;
+            warp_bisect(alpha, beta, k, warp == 0 ? 1 : k, lo, hi);
+            if ((threadIdx.x & 31) == 0) {
+                const double r = 0.5 * (lo + hi);
+                if (warp == 0) ctl.rmin = r; else ctl.rmax = r;
+                tridiag_eigenvector(alpha, beta, k, r, warp == 0 ? ymin : ymax);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double s1 = 0.0, s2 = 0.0;
+            for (int j = 0; j < k; ++j) {
+                const double vji = Vvec(j, m)[i];
+                s1 += ymin[j] * vji;
+                s2 += ymax[j] * vji;
+            }
+            vmin[i] = s1;
+            vmax[i] = s2;
+        }
+        __syncthreads();
+    }
+
+    // spectral_bounds (src/hydrodynamics.cpp:224-264). Updates the chain's
+    // warm-start vector in `cache` and ctl.lmin/lmax.
+    __device__ void spectral_bounds(double* cache, double* w, double* vmin, double* vmax, double* s) {
+        const bool can_warm = ctl.cache_valid != 0;
+        lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, cache, w, vmin, vmax);
+        if (can_warm && ctl.lz_steps < 4) {
+            lanczos(kLanczosCold, false, cache, w, vmin, vmax);
+            count(C_LZCOLD, 1);
+        } else {
+            count(can_warm ? C_LZWARM : C_LZCOLD, 1);
+        }
+        const double un = ch.seed_norm;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = vmin[i] + vmax[i] + 0.01 * a.seed_table[i] / un;
+        __syncthreads();
+        const double sn = sqrt(block_dot(s, s, n, red));
+        if (sn > 0.0 && isfinite(sn)) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) cache[i] = s[i] / sn;
+        }
+        if (threadIdx.x == 0) {
+            ctl.cache_valid = (sn > 0.0 && isfinite(sn)) ? 1 : 0;
+            double lmin = 0.5 * ctl.rmin;
+            const double lmax = 1.02 * ctl.rmax;
+            if (lmin < 1.0e-12) lmin = 1.0e-12;
+            if (lmin >= lmax) lmin = lmax * 1.0e-6;
+            ctl.lmin = lmin;
+            ctl.lmax = lmax;
+        }
+        __syncthreads();
+    }
+
+    // ---- Chebyshev square root (src/hydrodynamics.cpp:267-337) ----------
+    // out = D^{1/2} x0 approximation; returns with ctl.fd_err, ctl.L set.
+    // Scratch: Dx0, t1, t2, t3, Dv.
+    __device__ void chebyshev(const double* x0, double* out, double* Dx0, double* t1, double* t2, double* t3,
+                              double* Dv) {
+        apply_D(x0, Dx0);
+        __syncthreads();
+        const double x0Dx0 = block_dot(x0, Dx0, n, red);
+        const double lmin = ctl.lmin, lmax = ctl.lmax;
+        double Lr = sqrt(lmax / lmin) * ch.mult + 0.5;
+        int L;
+        if (!(Lr < 2.0e9)) L = kMaxCheb;  // guards the int conversion (NaN/huge)
+        else L = (int)Lr + 1;
+        L = L > kMaxCheb ? kMaxCheb : L;
+        L = L < 2 ? 2 : L;
+        const double da = 2.0 / (lmax - lmin);
+        const double db = -(lmax + lmin) / (lmax - lmin);
+        for (;;) {
+            // sqrt_chebyshev_coefficients (src/hydrodynamics.cpp:267-280)
+            for (int k = threadIdx.x; k <= L; k += blockDim.x)
+                sqx[k] = sqrt(cos(kPi * (k + 0.5) / (L + 1)) / da - db / da);
+            __syncthreads();
+            for (int j = threadIdx.x; j <= L; j += blockDim.x) {
+                double s = 0.0;
+                for (int k = 0; k <= L; ++k) s += sqx[k] * cos(j * (k + 0.5) * kPi / (L + 1));
+                s *= 2.0 / (L + 1);
+                if (j == 0) s /= 2.0;
+                coef[j] = s;
+            }
+            __syncthreads();
+            // chebyshev_series (src/hydrodynamics.cpp:284-312). T1 = da*D x0 + db*x0
+            // reuses D x0 from above (the same product, bit for bit).
+            const double c0 = coef[0], c1 = coef[1];
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const double tc = da * Dx0[i] + db * x0[i];
+                t1[i] = tc;
+                out[i] = c0 * x0[i];
+                out[i] += c1 * tc;
+            }
+            __syncthreads();
+            // three rotating buffers: T_{l-2} (x0 at first), T_{l-1}, T_l
+            double* T[3] = {t1, t2, t3};
+            const double* tp = x0;
+            int ic = 0, in = 1;
+            for (int l = 2; l <= L; ++l) {
+                const double* tc = T[ic];
+                double* tn = T[in];
+                apply_D(tc, Dv);
+                __syncthreads();
+                const double cl = coef[l];
+                for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                    double v = da * Dv[i] + db * tc[i];
+                    v = 2.0 * v - tp[i];
+                    tn[i] = v;
+                    out[i] += cl * v;
+                }
+                __syncthreads();
+                tp = tc;
+                const int nx = 3 - ic - in;
+                ic = in;
+                in = nx;
+            }
+            count(C_CHEB, L);
+            const double rr = block_dot(out, out, n, red);
+            const double fd = fabs(rr - x0Dx0) / x0Dx0;
+            if (fd <= ch.fd_tol || L >= kMaxCheb) {
+                if (threadIdx.x == 0) {
+                    ctl.fd_err = fd;
+                    ctl.L = L;
+                }
+                __syncthreads();
+                return;
+            }
+            const int grow = L / 4 > 1 ? L / 4 : 1;
+            L = (L + grow) > kMaxCheb ? kMaxCheb : L + grow;
+            __syncthreads();
+        }
+    }
+};
+
+// ------------------------------------------------------------ the kernel
+
+template <int FORM>
+__global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
+    extern __shared__ __align__(16) double sm[];
+    constexpr bool kMixed = (FORM == BDCU_FORM_MIXED_FP32);
+    const SmemLayout lay = smem_layout(a.n_max, a.d_in_smem, a.v_cap, kMixed);
+    const ScratchLayout scl = scratch_layout(a.n_max, a.d_in_smem, a.v_cap, a.need_chol, kMixed, a.need_d, a.need_lz);
+    Ctl& ctl = *reinterpret_cast<Ctl*>(sm + lay.ctl);
+    DevChain& ch = *reinterpret_cast<DevChain*>(sm + lay.chain);
+    double* scr = a.scratch + (int64_t)blockIdx.x * a.scratch_stride;
+
+    Block<FORM> B(a, ctl, ch);
+    B.red = sm + lay.red;
+    B.alpha = sm + lay.alpha;
+    B.beta = sm + lay.beta;
+    B.ymin = sm + lay.ymin;
+    B.ymax = sm + lay.ymax;
+    B.coef = sm + lay.coef;
+    B.sqx = sm + lay.sqx;
+    const int nvs = (int)round_up8(a.n_max);
+    for (int k = 0; k < kSlots; ++k) B.slot[k] = sm + lay.slots + (int64_t)k * nvs;
+    B.Vs = sm + lay.V;
+    B.Vg = scr + scl.V;
+    B.ldv = nvs;
+    B.Lt = scr + scl.Lt;
+    B.pos32 = reinterpret_cast<float4*>(sm + lay.f32);
+    B.vec32 = reinterpret_cast<float4*>(sm + lay.f32 + nvs);
+
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) ctl.chain = atomicAdd(a.work_counter, 1);
+        __syncthreads();
+        const int c = ctl.chain;
+        if (c >= a.n_chains) break;
+        {
+            const int nw = (int)(sizeof(DevChain) / 8);
+            const double* src = reinterpret_cast<const double*>(a.chains + c);
+            double* dst = reinterpret_cast<double*>(&ch);
+            for (int i = tid; i < nw; i += blockDim.x) dst[i] = src[i];
+        }
+        if (tid == 0) {
+            ctl.status = a.status[c];
+            ctl.cache_valid = (a.cache_mode == BDCU_CACHE_PERSIST) ? a.cache_valid[c] : 0;
+            for (int k = 0; k < 8; ++k) ctl.cnt[k] = 0;
+            ctl.brk = 0;
+        }
+        __syncthreads();
+        if (ctl.status & BDCU_ST_FATAL_MASK) {
+            __syncthreads();
+            continue;
+        }
+        if (ch.bad_param) {
+            if (tid == 0) a.status[c] = ctl.status | BDCU_ST_BAD_PARAM;
+            __syncthreads();
+            continue;
+        }
+        const int N = ch.N, n = 3 * N;
+        B.N = N;
+        B.n = n;
+        B.hi = ch.hstar > 0.0;
+        if constexpr (!kMixed) {
+            B.D = a.d_in_smem ? (sm + lay.D) : (scr + scl.D);
+            B.ldd = a.d_in_smem ? n : a.n_max;
+        } else {
+            B.D = nullptr;
+            B.ldd = 0;
+        }
+        double* R = B.slot[0];
+        double* Fs = B.slot[1];
+        double* Fe = B.slot[2];
+        double* dW = B.slot[3];
+        double* X0 = B.slot[4];
+        double* Rp = B.slot[5];
+        double* A = B.slot[6];
+        double* Bv = B.slot[7];
+        double* Cv = B.slot[8];
+        double* E = B.slot[9];
+        double* F = B.slot[10];
+        double* G = B.slot[11];
+        double* H = B.slot[12];
+        double* I = B.slot[13];
+        double* J = B.slot[14];
+        double* K = B.slot[15];
+        double* gR = a.R + 3 * ch.bead_off;
+        double* gcache = a.cache + 3 * ch.bead_off;
+        for (int i = tid; i < n; i += blockDim.x) R[i] = gR[i];
+        int32_t ix = 0, iy = 0, iseed = 0;
+        if (tid == 0) {
+            ix = a.rng[3 * c];
+            iy = a.rng[3 * c + 1];
+            iseed = a.rng[3 * c + 2];
+        }
+        const int nsteps = a.n_steps[c];
+        double t = a.t_start[c];
+        const double dt = ch.dt;
+        const double sqrt2inv = 1.0 / sqrt(2.0);
+        const double sqrt_dt = sqrt(dt);
+        __syncthreads();
+
+        for (int step = 0; step < nsteps; ++step) {
+            // recenter (src/integrator.cpp:88-93)
+            if (ch.update_com) {
+                if (tid < 3) {
+                    double s = 0.0;
+                    for (int i = 0; i < N; ++i) s = s + R[3 * i + tid];
+                    ctl.com[tid] = (1.0 / N) * s;
+                }
+                __syncthreads();
+                for (int i = tid; i < n; i += blockDim.x) R[i] = R[i] - ctl.com[i % 3];
+                __syncthreads();
+            }
+            if constexpr (kMixed) {
+                for (int b = tid; b < N; b += blockDim.x)
+                    B.pos32[b] = make_float4((float)R[3 * b], (float)R[3 * b + 1], (float)R[3 * b + 2], 0.f);
+            }
+            // Fs, Fe at R (src/integrator.cpp:105-111)
+            B.geometry(R, Cv, E);
+            __syncthreads();
+            B.spring_from_geometry(Cv, E, F, Fs);
+            __syncthreads();
+            B.explicit_force(R, t, Cv, E, F, G, Fe);
+            // The raw noise (src/mobility.cpp:18-29) and D at R (src/mobility.cpp:39-51):
+            // thread 0 draws the 3N uniforms, then joins the other threads, which
+            // have started assembling D.
+            if (tid == 0) {
+                if (iseed <= 0 || iy < 0) {
+                    const int32_t s = iseed < 0 ? -iseed : iseed;
+                    iy = (888889999 ^ s) | 1;
+                    ix = 777755555 ^ s;
+                    iseed = s + 1;
+                }
+                const float am = __fdiv_rn(__int_as_float(0x3f7fffff), 2147483648.0f);
+                uint32_t ux = (uint32_t)ix;
+                for (int k = 0; k < n; ++k) {
+                    ux ^= (ux << 13);
+                    ux ^= (ux >> 17);
+                    ux ^= (ux << 5);
+                    const int32_t kk = iy / 127773;
+                    iy = 16807 * (iy - kk * 127773) - 2836 * kk;
+                    if (iy < 0) iy += 2147483647;
+                    const uint32_t mixed = ux ^ (uint32_t)iy;
+                    const int32_t res = (int32_t)((mixed & 0x7fffffffu) | 1u);
+                    X0[k] = (double)__fmul_rn(am, __int2float_rn(res));
+                }
+                ix = (int32_t)ux;
+            }
+            if (B.hi) {
+                if constexpr (!kMixed) {
+                    B.build_rpy(R, B.D, B.ldd);
+                } else {
+                    if (ch.hi_method == BDCU_HI_CHOLESKY) {
+                        // dense FP64 D straight into the factor's storage (lower part)
+                        B.build_rpy(R, B.Lt, n);
+                    }
+                }
+            }
+            __syncthreads();
+            for (int i = tid; i < n; i += blockDim.x) {
+                const double y = X0[i] - 0.5;
+                X0[i] = (14.14855378 * y * y + 1.21569221) * y;
+            }
+            __syncthreads();
+            // brownian_step (src/mobility.cpp:58-88)
+            if (!B.hi) {
+                for (int i = tid; i < n; i += blockDim.x) dW[i] = sqrt_dt * X0[i];
+            } else if (ch.hi_method == BDCU_HI_CHOLESKY) {
+                bool ok;
+                if constexpr (!kMixed) ok = B.cholesky(B.D, B.ldd, false);
+                else ok = B.cholesky(nullptr, 0, true);
+                if (!ok) {
+                    if (tid == 0) ctl.status |= BDCU_ST_NOT_PD;
+                    __syncthreads();
+                    break;
+                }
+                B.lower_matvec(X0, A);
+                __syncthreads();
+                for (int i = tid; i < n; i += blockDim.x) dW[i] = sqrt_dt * A[i];
+            } else {
+                B.spectral_bounds(gcache, A, Bv, Cv, E);
+                B.chebyshev(X0, F, A, Bv, Cv, E, G);
+                if (!(ctl.fd_err <= ch.fd_tol)) {
+                    // Cholesky fallback (src/mobility.cpp:69-81)
+                    if (tid == 0) {
+                        ctl.status |= BDCU_ST_CHEB_FALLBACK;
+                        ctl.cnt[C_FALLBACK] += 1;
+                    }
+                    bool ok;
+                    if constexpr (!kMixed) {
+                        ok = B.cholesky(B.D, B.ldd, false);
+                    } else {
+                        B.build_rpy(R, B.Lt, n);
+                        ok = B.cholesky(nullptr, 0, true);
+                    }
+                    if (!ok) {
+                        if (tid == 0) ctl.status |= BDCU_ST_NOT_PD;
+                        __syncthreads();
+                        break;
+                    }
+                    B.lower_matvec(X0, F);
+                    __syncthreads();
+                }
+                for (int i = tid; i < n; i += blockDim.x) dW[i] = sqrt_dt * F[i];
+            }
+            __syncthreads();
+            // predictor (src/integrator.cpp:96-101)
+            double K1[9], K2[9];
+            kappa_at(ch, a.arena, t, K1);
+            kappa_at(ch, a.arena, t + dt, K2);
+            for (int i = tid; i < n; i += blockDim.x) A[i] = Fs[i] + Fe[i];
+            __syncthreads();
+            B.apply_D(A, Bv);
+            __syncthreads();
+            for (int i = tid; i < n; i += blockDim.x) {
+                const int r = i % 3, b3 = i - r;
+                const double fl1 = K1[3 * r] * R[b3] + K1[3 * r + 1] * R[b3 + 1] + K1[3 * r + 2] * R[b3 + 2];
+                Rp[i] = R[i] + dt * (fl1 + 0.25 * Bv[i]) + sqrt2inv * dW[i];
+            }
+            __syncthreads();
+            if constexpr (kMixed) {
+                // FP32 coordinates of R~ for the EV force at the predictor point
+                for (int b = tid; b < N; b += blockDim.x)
+                    B.pos32[b] = make_float4((float)Rp[3 * b], (float)Rp[3 * b + 1], (float)Rp[3 * b + 2], 0.f);
+            }
+            // upsilon (src/integrator.cpp:107-119)
+            B.geometry(Rp, E, F);
+            __syncthreads();
+            B.explicit_force(Rp, t + dt, E, F, G, H, Cv);
+            __syncthreads();
+            if constexpr (kMixed) {
+                // D stays the tensor at R (built once per step, src/integrator.cpp:113)
+                for (int b = tid; b < N; b += blockDim.x)
+                    B.pos32[b] = make_float4((float)R[3 * b], (float)R[3 * b + 1], (float)R[3 * b + 2], 0.f);
+                __syncthreads();
+            }
+            B.apply_D(Fs, A);
+            for (int i = tid; i < n; i += blockDim.x) E[i] = Fe[i] + Cv[i];
+            __syncthreads();
+            B.apply_D(E, F);
+            __syncthreads();
+            for (int i = tid; i < n; i += blockDim.x) {
+                const int r = i % 3, b3 = i - r;
+                const double fl1 = K1[3 * r] * R[b3] + K1[3 * r + 1] * R[b3 + 1] + K1[3 * r + 2] * R[b3 + 2];
+                const double fl2 = K2[3 * r] * Rp[b3] + K2[3 * r + 1] * Rp[b3 + 1] + K2[3 * r + 2] * Rp[b3 + 2];
+                const double flow = 0.5 * (fl1 + fl2);
+                Bv[i] = R[i] + dt * (flow + 0.125 * A[i] + 0.125 * F[i]) + sqrt2inv * dW[i];
+            }
+            __syncthreads();
+            // solve_connectors (src/integrator.cpp:125-165)
+            double* ups = Bv;
+            double* dups = Cv;
+            double* bond = E;
+            double* Rprev = G;
+            double* Fc = H;
+            double* Fb = I;
+            double* DFs = J;
+            double* Rc = K;
+            double* d2 = F;
+            for (int b = tid; b < N - 1; b += blockDim.x)
+                for (int d = 0; d < 3; ++d) {
+                    dups[3 * b + d] = ups[3 * (b + 1) + d] - ups[3 * b + d];
+                    bond[3 * b + d] = Rp[3 * (b + 1) + d] - Rp[3 * b + d];
+                }
+            for (int i = tid; i < n; i += blockDim.x) Rprev[i] = Rp[i];
+            __syncthreads();
+            const int max_iter = 100 * N;
+            int lstat = 0;
+            for (int iter = 0;; ++iter) {
+                for (int b = tid; b < N - 1; b += blockDim.x) {
+                    const double l = clamped_len(bond[3 * b], bond[3 * b + 1], bond[3 * b + 2]);
+                    const double f = connector_factor(ch, l);
+                    Fc[3 * b] = f * bond[3 * b];
+                    Fc[3 * b + 1] = f * bond[3 * b + 1];
+                    Fc[3 * b + 2] = f * bond[3 * b + 2];
+                }
+                __syncthreads();
+                B.bead_forces(Fc, Fb);
+                __syncthreads();
+                const double* DF = Fb;
+                if (B.hi) {
+                    B.apply_D(Fb, DFs);
+                    DF = DFs;
+                    __syncthreads();
+                }
+                const double c8 = 0.125 * dt, c4 = 0.25 * dt;
+                for (int b = tid; b < N - 1; b += blockDim.x) {
+                    double g[3], q[3];
+                    for (int d = 0; d < 3; ++d)
+                        g[d] = dups[3 * b + d] + c8 * (DF[3 * (b + 1) + d] - DF[3 * b + d]) + c4 * Fc[3 * b + d];
+                    solve_connector(g, dt, ch, q, lstat);
+                    bond[3 * b] = q[0];
+                    bond[3 * b + 1] = q[1];
+                    bond[3 * b + 2] = q[2];
+                }
+                __syncthreads();
+                if (tid < 3) {
+                    double acc = Rp[tid];
+                    Rc[tid] = acc;
+                    for (int b = 0; b < N - 1; ++b) {
+                        acc = acc + bond[3 * b + tid];
+                        Rc[3 * (b + 1) + tid] = acc;
+                    }
+                }
+                __syncthreads();
+                for (int i = tid; i < N; i += blockDim.x) {
+                    const double e0 = Rc[3 * i] - Rprev[3 * i], e1 = Rc[3 * i + 1] - Rprev[3 * i + 1],
+                                 e2 = Rc[3 * i + 2] - Rprev[3 * i + 2];
+                    d2[i] = e0 * e0 + e1 * e1 + e2 * e2;
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    double s = 0.0;
+                    for (int i = 0; i < N; ++i) s += d2[i];
+                    ctl.incr = sqrt(s) / N;
+                    ctl.cnt[C_CORR] += 1;
+                    int verdict = 0;  // 0 continue, 1 converged, 2 cap reached, 3 non-finite
+                    if (ctl.incr < ch.tol) verdict = 1;
+                    else if (!(ctl.incr == ctl.incr) || isinf(ctl.incr)) verdict = 3;
+                    else if (iter >= max_iter) verdict = 2;
+                    ctl.brk = verdict;
+                }
+                __syncthreads();
+                const int verdict = ctl.brk;
+                if (verdict != 0) {
+                    __syncthreads();
+                    if (tid == 0) {
+                        ctl.brk = 0;
+                        if (verdict == 2) {
+                            ctl.status |= BDCU_ST_NONCONVERGED;
+                            ctl.cnt[C_NONCONV] += 1;
+                        }
+                        if (verdict == 3) ctl.status |= BDCU_ST_NONFINITE;
+                    }
+                    __syncthreads();
+                    break;
+                }
+                for (int i = tid; i < n; i += blockDim.x) Rprev[i] = Rc[i];
+                __syncthreads();
+            }
+            if (lstat) atomicOr(&ctl.status, lstat);
+            __syncthreads();
+            if (ctl.status & BDCU_ST_FATAL_MASK) break;
+            for (int i = tid; i < n; i += blockDim.x) R[i] = Rc[i];
+            if (tid == 0) ctl.cnt[C_STEPS] += 1;
+            t += dt;
+            __syncthreads();
+        }
+        __syncthreads();
+        // write back: positions (unless the chain failed), RNG, cache flag, status, counters
+        if (!(ctl.status & BDCU_ST_FATAL_MASK))
+            for (int i = tid; i < n; i += blockDim.x) gR[i] = R[i];
+        if (tid == 0) {
+            a.rng[3 * c] = ix;
+            a.rng[3 * c + 1] = iy;
+            a.rng[3 * c + 2] = iseed;
+            a.cache_valid[c] = ctl.cache_valid;
+            a.status[c] = ctl.status;
+            int64_t* cc = reinterpret_cast<int64_t*>(a.counters + c);
+            for (int k = 0; k < 8; ++k) cc[k] += ctl.cnt[k];
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace bdcu

@@ -1,0 +1,184 @@
+"""Device-side engine over the C ABI (include/bdsim_cuda.h).
+
+`Context` wraps one bdcu_ctx. `Ensemble` keeps a batch of chains resident on
+the GPU -- positions, RNG streams, spectral warm-start vectors, status and
+counters in torch device tensors -- and advances them chunk by chunk, which is
+how `simulate` / `run_ensemble` use it. PyTorch provides the device buffers
+and the stream; every computation is a CUDA kernel of libbdsim_cuda.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import (BdcuCounters, CACHE_PERSIST, CACHE_RESET_PER_CALL, COUNTER_FIELDS, FORM_MIXED_FP32,
+                   FORM_PLAIN_FP64, ST_FATAL_MASK, dptr)
+
+FORMS = {"plain": FORM_PLAIN_FP64, "fp64": FORM_PLAIN_FP64, "mixed": FORM_MIXED_FP32, "fp32": FORM_MIXED_FP32,
+         FORM_PLAIN_FP64: FORM_PLAIN_FP64, FORM_MIXED_FP32: FORM_MIXED_FP32}
+
+
+def form_code(form) -> int:
+    try:
+        return FORMS[form]
+    except KeyError:
+        raise ValueError(f"unknown integrator form {form!r} (use 'plain' or 'mixed')") from None
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("bdsim_b200 needs a CUDA device (B200); none is visible. There is no CPU fallback.")
+    return torch
+
+
+class BdcuError(RuntimeError):
+    pass
+
+
+class Context:
+    """One C-ABI context on `device`, bound to the current torch stream."""
+
+    def __init__(self, device: int = 0):
+        torch = _torch()
+        self.lib = _abi.load_library()
+        self.device = int(device)
+        self.torch = torch
+        h = ctypes.c_void_p()
+        rc = self.lib.bdcu_create(self.device, ctypes.byref(h))
+        if rc != 0:
+            raise BdcuError(f"bdcu_create failed ({rc})")
+        self.h = h
+        self.n_chains = 0
+        self.n_beads = []
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.bdcu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            msg = self.lib.bdcu_last_error(self.h).decode(errors="replace")
+            raise BdcuError(f"{what} failed ({rc}): {msg}")
+
+    def use_stream(self, stream=None):
+        torch = self.torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        self._ck(self.lib.bdcu_set_stream(self.h, ctypes.c_void_p(s.cuda_stream)), "bdcu_set_stream")
+
+    def set_chains(self, phys_list, sim_list, n_beads_list):
+        prec, srec, arena = _abi.pack_batch(phys_list, sim_list, n_beads_list)
+        self._arena = arena
+        self._ck(self.lib.bdcu_set_chains(self.h, len(phys_list), prec, srec,
+                                          arena.ctypes.data_as(_abi.c_double_p), arena.size),
+                 "bdcu_set_chains")
+        self.n_chains = len(phys_list)
+        self.n_beads = list(n_beads_list)
+
+    def run(self, R, rng, cache, cache_valid, t_start, n_steps, status, counters, form, cache_mode):
+        self.use_stream()
+        self._ck(self.lib.bdcu_run(self.h, dptr(R), dptr(rng), dptr(cache), dptr(cache_valid), dptr(t_start),
+                                   dptr(n_steps), dptr(status), dptr(counters), int(form), int(cache_mode)),
+                 "bdcu_run")
+
+    def integrate_host(self, R_host: np.ndarray, rng_host: np.ndarray, form):
+        """Host-buffer integrate over each chain's SimParams span (cold cache).
+        R_host (total_beads, 3) float64 and rng_host (n, 3) int32 are updated
+        in place. Returns (status int32[n], counters list of dicts)."""
+        self.use_stream()
+        status = np.zeros(self.n_chains, dtype=np.int32)
+        cnt = (BdcuCounters * self.n_chains)()
+        self._ck(self.lib.bdcu_integrate_host(self.h, R_host.ctypes.data_as(_abi.c_double_p),
+                                              rng_host.ctypes.data_as(_abi.c_int32_p),
+                                              status.ctypes.data_as(_abi.c_int32_p), cnt, int(form)),
+                 "bdcu_integrate_host")
+        return status, [{f: getattr(c, f) for f in COUNTER_FIELDS} for c in cnt]
+
+    def total_force(self, R_dev, F_dev):
+        self.use_stream()
+        self._ck(self.lib.bdcu_total_force(self.h, dptr(R_dev), dptr(F_dev)), "bdcu_total_force")
+
+    def forces(self, R_dev, F_dev, which: int, t: float = 0.0):
+        self.use_stream()
+        self._ck(self.lib.bdcu_forces(self.h, dptr(R_dev), float(t), int(which), dptr(F_dev)), "bdcu_forces")
+
+    def ran1(self, rng_dev, n_per_chain: int, out_dev):
+        self.use_stream()
+        self._ck(self.lib.bdcu_ran1(self.h, int(rng_dev.shape[0]), dptr(rng_dev), int(n_per_chain),
+                                    dptr(out_dev)), "bdcu_ran1")
+
+
+class Ensemble:
+    """A batch of independent chains resident on one GPU.
+
+    phys_list/sim_list: one PhysParams/SimParams per chain (sim supplies dt,
+    implicit_loop_tol and update_center_of_mass; the time span of each
+    `advance` is given explicitly). R0_list: (N_i, 3) arrays. rng_states:
+    (ix, iy, seed) per chain.
+    """
+
+    def __init__(self, phys_list, sim_list, R0_list, rng_states, device: int = 0, form="plain"):
+        torch = _torch()
+        self.torch = torch
+        self.form = form_code(form)
+        self.ctx = Context(device)
+        self.n = len(R0_list)
+        self.Ns = [int(len(r)) for r in R0_list]
+        self.ctx.set_chains(phys_list, sim_list, self.Ns)
+        self.sims = list(sim_list)
+        self.offsets = np.zeros(self.n + 1, dtype=np.int64)
+        self.offsets[1:] = np.cumsum(self.Ns)
+        dev = torch.device("cuda", device)
+        self.dev = dev
+        R = np.ascontiguousarray(np.concatenate([np.asarray(r, dtype=np.float64).reshape(-1, 3) for r in R0_list]))
+        self.R = torch.from_numpy(R).to(dev)
+        self.rng = torch.tensor(np.asarray(rng_states, dtype=np.int32).reshape(self.n, 3), device=dev)
+        self.cache = torch.zeros(3 * int(self.offsets[-1]), dtype=torch.float64, device=dev)
+        self.cache_valid = torch.zeros(self.n, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(self.n, dtype=torch.int32, device=dev)
+        self.counters = torch.zeros((self.n, len(COUNTER_FIELDS)), dtype=torch.int64, device=dev)
+        self._t = torch.zeros(self.n, dtype=torch.float64, device=dev)
+        self._k = torch.zeros(self.n, dtype=torch.int32, device=dev)
+
+    def advance(self, t_start, n_steps, cache_mode=CACHE_PERSIST):
+        """Run n_steps[i] steps of chain i from time t_start[i] (asynchronous)."""
+        torch = self.torch
+        self._t.copy_(torch.as_tensor(np.broadcast_to(np.asarray(t_start, dtype=np.float64), (self.n,)).copy()))
+        self._k.copy_(torch.as_tensor(np.broadcast_to(np.asarray(n_steps, dtype=np.int32), (self.n,)).copy()))
+        self.ctx.run(self.R, self.rng, self.cache, self.cache_valid, self._t, self._k, self.status,
+                     self.counters, self.form, cache_mode)
+
+    def reset_cache(self):
+        self.cache_valid.zero_()
+
+    def positions(self):
+        R = self.R.cpu().numpy()
+        return [R[self.offsets[i]:self.offsets[i + 1]].copy() for i in range(self.n)]
+
+    def total_force(self):
+        F = self.torch.empty_like(self.R)
+        self.ctx.total_force(self.R, F)
+        Fh = F.cpu().numpy()
+        return [Fh[self.offsets[i]:self.offsets[i + 1]].copy() for i in range(self.n)]
+
+    def rng_states(self):
+        return [tuple(int(v) for v in row) for row in self.rng.cpu().numpy()]
+
+    def statuses(self) -> np.ndarray:
+        return self.status.cpu().numpy()
+
+    def failed(self) -> np.ndarray:
+        return (self.statuses() & ST_FATAL_MASK) != 0
+
+    def counter_totals(self) -> dict:
+        c = self.counters.sum(dim=0).cpu().numpy()
+        return {f: int(v) for f, v in zip(COUNTER_FIELDS, c)}

@@ -1,0 +1,232 @@
+/*
+ * bdsim_cuda.h -- C ABI of the B200 ensemble integrator for bdsim's
+ * ChainIntegrator step.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * an int status (BDCU_OK == 0; otherwise a BDCU_E_* code, with a message from
+ * bdcu_last_error). No C++ exception crosses this boundary.
+ *
+ * What each entry point replaces in the reference (paths relative to the
+ * bdsim project root):
+ *
+ *   bdcu_integrate_host   _bdsim.integrate(R, phys, sim, rng)
+ *                         bindings/module.cpp:45-50  ->  time_integrate_chain
+ *                         src/integrator.hpp:32, src/integrator.cpp:209-212
+ *                         (batched: many chains, one call; the RNG state and
+ *                         R are updated in place exactly as the reference
+ *                         mutates its Rng and returns the evolved R)
+ *   bdcu_run              the same step loop on device-resident state
+ *                         (ChainIntegrator::run, src/integrator.cpp:101-120)
+ *   bdcu_total_force      _bdsim.total_force(R, phys)
+ *                         bindings/module.cpp:67-76
+ *   bdcu_forces           _bdsim.spring_force / ev_force / bending_force /
+ *                         external_force, bindings/module.cpp:52-66,128-132
+ *   bdcu_ran1             Rng::ran_1, src/rng.cpp:41-70 (per-chain streams)
+ *   bdcu_set_chains       PhysParams / SimParams marshalling
+ *                         (src/model.hpp:20-35, src/integrator.hpp:22-28,
+ *                         pickled state tuples bindings/module.cpp:184-297)
+ *
+ * Parameter layout. One bdcu_phys and one bdcu_sim per chain. Variable-size
+ * tables (flow samples, external-force samples, SDK phi) live in one double
+ * "arena" the caller passes alongside, addressed by index:
+ *
+ *   flow table      arena[flow_offset .. +n)           sample times (ascending)
+ *                   arena[flow_offset+n .. +9n)        row-major kappa per sample
+ *   external list   ext_n_entries records starting at arena[ext_offset], each
+ *                   [bead, is_constant, fx, fy, fz, n_times,
+ *                    t_0 .. t_{n-1}, f_0x f_0y f_0z .. f_{n-1}z]
+ *                   (6 + 4*n_times doubles); negative bead counts from the end
+ *   SDK phi         arena[phi_offset .. + N*N) row-major, or phi_offset == -1
+ */
+#ifndef BDSIM_CUDA_H
+#define BDSIM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums: same numeric values as the reference (src/types.hpp:27-55) ---- */
+enum {
+    BDCU_SPRING_HOOK = 1,
+    BDCU_SPRING_FENE = 2,
+    BDCU_SPRING_ILC = 3,
+    BDCU_SPRING_WLC = 4,
+    BDCU_SPRING_FRAENKEL = 5,
+    BDCU_SPRING_FENE_FRAENKEL = 6,
+    BDCU_SPRING_WLC_BOUNDED = 7
+};
+enum { BDCU_EV_NONE = 0, BDCU_EV_GAUSS = 1, BDCU_EV_LJ = 2, BDCU_EV_SDK = 3, BDCU_EV_SDK_STICKERS = 4 };
+enum { BDCU_BEND_NONE = 0, BDCU_BEND_ONE_MINUS_COS = 1 };
+enum { BDCU_HI_CHEBYSHEV = 0, BDCU_HI_CHOLESKY = 1, BDCU_HI_EXACT_SQRT = 2 };
+
+/* ---- integrator forms ---- */
+enum {
+    /* FP64, the reference algorithm step for step, one chain per thread block. */
+    BDCU_FORM_PLAIN_FP64 = 0,
+    /* FP32 matrix-free RPY products and FP32 excluded volume; FP64 positions,
+       connector solve, Lanczos bounds and Cholesky. */
+    BDCU_FORM_MIXED_FP32 = 1
+};
+
+/* ---- spectral-cache policy across calls ---- */
+enum {
+    /* the reference: each integrate call starts Lanczos cold
+       (src/integrator.cpp:211 builds a fresh PhysicalModel per call) */
+    BDCU_CACHE_RESET_PER_CALL = 0,
+    /* keep the warm-start vector across calls (a chunked run then equals one
+       continuous call of the reference) */
+    BDCU_CACHE_PERSIST = 1
+};
+
+/* ---- per-chain status bits (device word per chain) ---- */
+enum {
+    BDCU_ST_NONCONVERGED = 1,  /* corrector hit 100N iterations; step accepted
+                                  (src/integrator.cpp:195-198) */
+    BDCU_ST_NOT_PD = 2,        /* Cholesky pivot <= 0; chain stopped
+                                  (src/linalg.cpp:16-25,99) */
+    BDCU_ST_CHEB_FALLBACK = 4, /* Chebyshev FD check failed, Cholesky used
+                                  (src/mobility.cpp:69-81) */
+    BDCU_ST_RTSAFE_FAIL = 8,   /* rtsafe bracket/iteration failure; chain
+                                  stopped (the reference aborts,
+                                  src/numerics.hpp:31-36,72) */
+    BDCU_ST_NONFINITE = 16,    /* positions became NaN/Inf; chain stopped */
+    BDCU_ST_BAD_PARAM = 32     /* WLCbounded sigma>1 or ExactSqrt; chain
+                                  stopped (reference aborts) */
+};
+#define BDCU_ST_FATAL_MASK (BDCU_ST_NOT_PD | BDCU_ST_RTSAFE_FAIL | BDCU_ST_NONFINITE | BDCU_ST_BAD_PARAM)
+
+/* ---- error codes returned by entry points ---- */
+enum {
+    BDCU_OK = 0,
+    BDCU_E_ARG = 1,      /* invalid argument */
+    BDCU_E_CUDA = 2,     /* CUDA runtime error */
+    BDCU_E_STATE = 3,    /* call order (e.g. run before set_chains) */
+    BDCU_E_NOMEM = 4,    /* allocation failed */
+    BDCU_E_LIMIT = 5     /* size beyond a documented maximum */
+};
+
+/* PhysParams (src/model.hpp:20-35) with its SpringParams (src/spring.hpp:12-19),
+   EVParams (src/excluded_volume.hpp:17-25), BendingParams (src/bending.hpp:9-12),
+   Flow (src/flow.hpp:17-43) and ExternalForce (src/external_force.hpp:32-57). */
+typedef struct bdcu_phys {
+    int32_t n_beads;
+    int32_t spring_type;
+    double sqrtb;
+    double natural_length;
+    int32_t ev_type;
+    int32_t contour_dist_for_ev;
+    double zstar;
+    double dstar;
+    double min_cutoff;
+    double max_cutoff;
+    int64_t phi_offset;
+    int32_t bend_type;
+    int32_t equilibration;
+    double bend_stiffness;
+    double hstar;
+    int32_t hi_method;
+    int32_t flow_n_times;
+    double ncheb_multiplier;
+    double fd_err_max;
+    double flow_kappa[9];
+    int64_t flow_offset;
+    int32_t ext_n_entries;
+    int32_t reserved0;
+    int64_t ext_offset;
+} bdcu_phys;
+
+/* SimParams (src/integrator.hpp:22-28). time_start/time_end bound the step
+   loop exactly as ChainIntegrator::run does (src/integrator.cpp:102). */
+typedef struct bdcu_sim {
+    double time_start;
+    double time_end;
+    double dt;
+    double implicit_loop_tol;
+    int32_t update_center_of_mass;
+    int32_t reserved0;
+} bdcu_sim;
+
+/* Per-chain counters (device). They replace the reference's only in-code
+   counters, SpectralCache::cold_runs/warm_runs (src/hydrodynamics.hpp:33-37),
+   and its global nonconvergence_count (src/integrator.cpp:60). */
+typedef struct bdcu_counters {
+    int64_t steps;            /* integrator steps completed */
+    int64_t dx_products;      /* D.x products (the dominant work unit) */
+    int64_t cheb_terms;       /* sum of Chebyshev term counts L over attempts */
+    int64_t corrector_iters;  /* implicit-corrector iterations */
+    int64_t lanczos_cold;
+    int64_t lanczos_warm;
+    int64_t cheb_fallbacks;   /* FD failures that fell back to Cholesky */
+    int64_t nonconverged;     /* steps whose corrector did not converge */
+} bdcu_counters;
+
+typedef struct bdcu_ctx bdcu_ctx;
+
+/* Library version string. */
+const char* bdcu_version(void);
+
+/* Create a context on CUDA device `device`. Allocates nothing on the device. */
+int bdcu_create(int device, bdcu_ctx** out);
+int bdcu_destroy(bdcu_ctx* ctx);
+/* Stream for all subsequent work (a cudaStream_t; NULL = legacy default). */
+int bdcu_set_stream(bdcu_ctx* ctx, void* stream);
+/* Message of the last failing call on this context (NUL-terminated). */
+const char* bdcu_last_error(bdcu_ctx* ctx);
+
+/* Describe the chains of the batch. phys/sim: n_chains records (host).
+   arena: arena_len doubles (host). Derived constants are computed here on the
+   host (pow/exp as the reference's constructors do) and uploaded. */
+int bdcu_set_chains(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys,
+                    const bdcu_sim* sim, const double* arena, int64_t arena_len);
+
+/* Number of integrator steps the reference loop
+   `for (t = time_start; t <= time_end + dt/2; t += dt)` takes for chain i.
+   Host-side, no device work. */
+int bdcu_count_steps(const bdcu_sim* sim, int64_t* n_steps_out);
+
+/* Run the step loop on device-resident state, asynchronously on the context
+   stream. All pointers are device pointers owned by the caller:
+     R            total_beads*3 doubles, chains concatenated in set_chains order
+     rng          n_chains*3 int32 (ix, iy, seed), advanced in place
+     cache        total_beads*3 doubles, spectral warm-start vectors
+     cache_valid  n_chains int32 (0 => next Lanczos is cold)
+     t_start      n_chains doubles, first step time of this call
+     n_steps      n_chains int32, steps to take in this call
+     status       n_chains int32, OR-ed with BDCU_ST_* bits
+     counters     n_chains bdcu_counters, accumulated
+   A chain whose status has a fatal bit set is skipped. */
+int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache,
+             int32_t* cache_valid, const double* t_start, const int32_t* n_steps,
+             int32_t* status, bdcu_counters* counters, int form, int cache_mode);
+
+/* The reference-facing batched integrate: host R (total_beads*3), host rng
+   (n_chains*3), host status (n_chains). Runs every chain over its own
+   bdcu_sim [time_start, time_end] with a cold spectral cache, as
+   time_integrate_chain does; copies R, rng and status back. Synchronous. */
+int bdcu_integrate_host(bdcu_ctx* ctx, double* R_host, int32_t* rng_host,
+                        int32_t* status_host, bdcu_counters* counters_host,
+                        int form);
+
+/* Intramolecular force (spring + EV + bending, no external) at R (device
+   pointers, total_beads*3 each), FP64. */
+int bdcu_total_force(bdcu_ctx* ctx, const double* R, double* F);
+
+/* Force components at R: `which` ORs BDCU_F_* bits. A single bit gives that
+   force alone (bindings/module.cpp:52-66,128-132: spring_force, ev_force,
+   bending_force, external_force at time t); several bits are summed as
+   (spring + (EV + bending)) + external, the reference's grouping. */
+enum { BDCU_F_SPRING = 1, BDCU_F_EV = 2, BDCU_F_BEND = 4, BDCU_F_EXTERNAL = 8 };
+int bdcu_forces(bdcu_ctx* ctx, const double* R, double t, int which, double* F);
+
+/* Draw n_per_chain uniforms per chain from device RNG states (n_chains*3
+   int32, advanced in place) into out (device, n_chains*n_per_chain). */
+int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BDSIM_CUDA_H */
