@@ -1,0 +1,257 @@
+"""The run layer of bdsim (python/bdsim/ensemble.py of the bdsim project) with
+backend="cuda": every trajectory of an ensemble is a chain of one device
+batch, advanced on the GPU chunk by chunk.
+
+Semantics kept from the reference:
+  * trajectory i is seeded seed+i and starts from INITIALIZERS[method](N, seed+i)
+    (ensemble.py:197-199, 216-220);
+  * a chunk of k steps is one integrate call over [t0, t0+(k-1)dt], and each
+    call starts the spectral (Lanczos) cache cold (ensemble.py:165-182);
+  * snapshots at step 0, every write_every steps and the last step;
+  * a trajectory whose integration fails becomes a Failure, dropped and
+    reported, with MAX_FAILED_FRACTION enforced (ensemble.py:289-343).
+"""
+from __future__ import annotations
+
+import os
+import sys
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import storage
+from ._abi import CACHE_PERSIST, CACHE_RESET_PER_CALL, ST_FATAL_MASK, count_steps
+from .core import IntegratorError, integrate
+from .engine import Ensemble
+from .initial import (fene_fraenkel_bending_chain, fene_fraenkel_chain, fene_fraenkel_chain_aligned_x,
+                      gaussian_chain)
+from .parallel import Failure
+from .params import PhysParams, Rng, SimParams
+
+
+def _init_gaussian(n, seed, kw): return gaussian_chain(n, seed=seed, **kw)
+def _init_fene_fraenkel(n, seed, kw): return fene_fraenkel_chain(n, seed=seed, **kw)
+def _init_fene_fraenkel_x(n, seed, kw): return fene_fraenkel_chain_aligned_x(n, seed=seed, **kw)
+def _init_fene_fraenkel_bending(n, seed, kw): return fene_fraenkel_bending_chain(n, seed=seed, **kw)
+
+
+INITIALIZERS = {
+    "gaussian": _init_gaussian,
+    "fene_fraenkel": _init_fene_fraenkel,
+    "fene_fraenkel_x": _init_fene_fraenkel_x,
+    "fene_fraenkel_bending": _init_fene_fraenkel_bending,
+}
+
+MAX_FAILED_FRACTION = 0.1
+
+
+@dataclass
+class Initial:
+    """Initial-configuration method (a key of INITIALIZERS) and its kwargs."""
+    method: str = "gaussian"
+    kwargs: dict = field(default_factory=dict)
+
+
+@dataclass
+class Output:
+    """Run directory, snapshot interval (0 => start and end only), forces flag."""
+    directory: str = None
+    write_every: int = 0
+    write_forces: bool = False
+    compression: str = "gzip"
+
+
+def _segment(sim: SimParams, t0: float, t1: float) -> SimParams:
+    s = SimParams()
+    s.dt = sim.dt
+    s.implicit_loop_tol = sim.implicit_loop_tol
+    s.update_center_of_mass = sim.update_center_of_mass
+    s.time_start = t0
+    s.time_end = t1
+    return s
+
+
+def n_steps_of(sim: SimParams) -> int:
+    """Integrator steps implied by sim's time span and dt (ensemble.py:154-156)."""
+    return int(round((sim.time_end - sim.time_start) / sim.dt))
+
+
+def mean_stderr(values):
+    arr = np.asarray(values, dtype=float)
+    n = arr.size
+    mean = float(arr.mean())
+    stderr = float(arr.std(ddof=1) / np.sqrt(n)) if n > 1 else float("nan")
+    return mean, stderr
+
+
+def _phys_summary(phys: PhysParams) -> dict:
+    return {"n_beads": int(phys.number_of_beads), "spring_type": str(phys.spring.type),
+            "sqrtb": float(phys.spring.sqrtb), "natural_length": float(phys.spring.natural_length),
+            "hstar": float(phys.hstar), "hi_method": str(phys.hi_method)}
+
+
+def _drop_failures(results, what, max_fraction=None):
+    ok = [r for r in results if not isinstance(r, Failure)]
+    bad = [r for r in results if isinstance(r, Failure)]
+    if not bad:
+        return ok, bad
+    n = len(results)
+    frac = len(bad) / n
+    seen, lines = set(), []
+    for f in bad:
+        key = f.message.split("(")[0]
+        if key not in seen:
+            seen.add(key)
+            lines.append(f"    trajectory {f.index}: {f.message.splitlines()[0]}")
+    print(f"bdsim: {len(bad)} of {n} {what} failed and were dropped ({100 * frac:.0f}%). Distinct causes:",
+          file=sys.stderr)
+    for line in lines[:3]:
+        print(line, file=sys.stderr)
+    limit = MAX_FAILED_FRACTION if max_fraction is None else max_fraction
+    if frac > limit:
+        raise RuntimeError(f"{len(bad)} of {n} {what} failed ({100 * frac:.0f}%), above the {100 * limit:.0f}% "
+                           "limit. Reduce dt or tighten implicit_loop_tol, or raise max_failed_fraction.")
+    if not ok:
+        raise RuntimeError(f"every one of the {n} {what} failed")
+    return ok, bad
+
+
+def _check_backend(backend):
+    if backend != "cuda":
+        raise ValueError(f"bdsim_b200 runs ensembles on the GPU: use backend='cuda' (got {backend!r})")
+
+
+def _start(phys, sim, n_traj, seed, initial, form, device):
+    initial = initial or Initial()
+    R0s = [INITIALIZERS[initial.method](phys.number_of_beads, seed + i, dict(initial.kwargs)) for i in range(n_traj)]
+    rngs = [Rng(seed + i).state() for i in range(n_traj)]
+    return Ensemble([phys] * n_traj, [sim] * n_traj, R0s, rngs, device=device, form=form), R0s
+
+
+def simulate(phys: PhysParams, sim: SimParams, *, n_traj: int = 1, seed: int = 0, n_steps: int = None,
+             initial: Initial = None, output: Output = None, backend: str = "cuda", n_workers: int = None,
+             on_error: str = "skip", max_failed_fraction: float = None, form="plain", device: int = 0):
+    """Run n_traj chains on the GPU and write their snapshots (ensemble.py:238-277)."""
+    _check_backend(backend)
+    initial = initial or Initial()
+    output = output or Output()
+    if output.directory is None:
+        raise ValueError("output.directory must be set (the run folder to write into)")
+    n_steps = int(n_steps) if n_steps is not None else n_steps_of(sim)
+    os.makedirs(output.directory, exist_ok=True)
+    ens, R0s = _start(phys, sim, n_traj, seed, initial, form, device)
+    w = output.write_every if (output.write_every and output.write_every > 0) else n_steps
+    snaps_R, snaps_F, steps, times = [np.stack(R0s)], [], [0], [sim.time_start]
+    if output.write_forces:
+        snaps_F.append(np.stack(ens.total_force()))
+    step = 0
+    while step < n_steps:
+        chunk = min(w, n_steps - step)
+        t0 = sim.time_start + step * sim.dt
+        k = count_steps(_segment(sim, t0, t0 + (chunk - 1) * sim.dt))
+        ens.advance(t0, k, CACHE_RESET_PER_CALL)
+        step += chunk
+        steps.append(step)
+        times.append(sim.time_start + step * sim.dt)
+        snaps_R.append(np.stack(ens.positions()))
+        if output.write_forces:
+            snaps_F.append(np.stack(ens.total_force()))
+    status = ens.statuses()
+    sink = storage.SnapshotSink()
+    results = []
+    P = np.stack(snaps_R, axis=1)  # (n_traj, n_snap, N, 3)
+    Fa = np.stack(snaps_F, axis=1) if output.write_forces else None
+    for i in range(n_traj):
+        if status[i] & ST_FATAL_MASK:
+            results.append(Failure(i, IntegratorError(int(status[i]), i)))
+            continue
+        attrs = {"index": i, "seed": seed + i, "n_steps": n_steps, "write_every": output.write_every or n_steps,
+                 "dt": float(sim.dt), **{f"phys_{k}": v for k, v in _phys_summary(phys).items()}}
+        path = storage.trajectory_path(output.directory, i)
+        sink.put(path, steps=steps, times=times, positions=P[i], forces=None if Fa is None else Fa[i],
+                 attrs=attrs, compression=output.compression)
+        results.append(os.path.basename(path))
+    sink.close()
+    if on_error == "raise":
+        bad = [r for r in results if isinstance(r, Failure)]
+        if bad:
+            raise bad[0].error
+    files, failed = _drop_failures(results, "trajectories", max_failed_fraction)
+    storage.write_manifest(output.directory, {
+        "n_trajectories": len(files), "n_trajectories_requested": n_traj, "n_trajectories_failed": len(failed),
+        "seed": seed, "n_steps": n_steps, "dt": float(sim.dt), "write_every": output.write_every or n_steps,
+        "write_forces": bool(output.write_forces), "initial": {"method": initial.method, "kwargs": initial.kwargs},
+        "phys": _phys_summary(phys), "files": list(files), "backend": "cuda", "form": str(form),
+        "counters": ens.counter_totals()})
+    return storage.read_run(output.directory)
+
+
+def trajectory_samples(R0, phys: PhysParams, sim: SimParams, rng, sample_times, *, form="plain", device=0):
+    """Configurations of one chain at each sample time (ensemble.py:126-138)."""
+    R = np.asarray(R0, dtype=np.float64)
+    out, t = [], sim.time_start
+    for ts in sample_times:
+        R = integrate(R, phys, _segment(sim, t, ts), rng, form=form, device=device)
+        out.append((ts, R.copy()))
+        t = ts
+    return out
+
+
+def final_state(R0, phys, sim, rng):
+    """per_trajectory reducer: the final (N,3) configuration (ensemble.py:309-318)."""
+    return np.asarray(integrate(R0, phys, sim, rng), dtype=np.float64)
+
+
+def sampled_states(R0, phys, sim, rng, sample_times):
+    """per_trajectory reducer: the configuration at each sample time (ensemble.py:321-327)."""
+    return [R for _t, R in trajectory_samples(R0, phys, sim, rng, sample_times)]
+
+
+def run_ensemble(phys: PhysParams, sim: SimParams, n_traj: int, per_trajectory, *, args=(), seed: int = 0,
+                 initial: Initial = None, backend="cuda", n_workers=None, on_error="skip",
+                 max_failed_fraction=None, form="plain", device: int = 0):
+    """Run n_traj chains, reducing each with per_trajectory (ensemble.py:330-379).
+
+    final_state and sampled_states run batched: all trajectories advance
+    together in one device batch per integrate segment. Any other function is
+    called once per trajectory as per_trajectory(R0, phys, sim, rng, *args);
+    the integrate calls it makes run on the GPU one chain at a time.
+    """
+    _check_backend(backend)
+    initial = initial or Initial()
+    if per_trajectory is final_state or per_trajectory is sampled_states:
+        ens, _ = _start(phys, sim, n_traj, seed, initial, form, device)
+        if per_trajectory is final_state:
+            segs = [(sim.time_start, sim.time_end)]
+        else:
+            times = list(args[0])
+            segs = list(zip([sim.time_start] + times[:-1], times))
+        per = [[] for _ in range(n_traj)]
+        for t0, t1 in segs:
+            k = count_steps(_segment(sim, t0, t1))
+            ens.advance(t0, k, CACHE_RESET_PER_CALL)
+            for i, R in enumerate(ens.positions()):
+                per[i].append(R)
+        status = ens.statuses()
+        out = []
+        for i in range(n_traj):
+            if status[i] & ST_FATAL_MASK:
+                out.append(Failure(i, IntegratorError(int(status[i]), i)))
+            else:
+                out.append(per[i][-1] if per_trajectory is final_state else per[i])
+    else:
+        out = []
+        for i in range(n_traj):
+            R0 = INITIALIZERS[initial.method](phys.number_of_beads, seed + i, dict(initial.kwargs))
+            try:
+                out.append(per_trajectory(R0, phys, sim, Rng(seed + i), *args))
+            except Exception as exc:
+                if on_error == "raise":
+                    raise
+                out.append(Failure(i, exc))
+    if on_error == "raise":
+        bad = [r for r in out if isinstance(r, Failure)]
+        if bad:
+            raise bad[0].error
+    out, _ = _drop_failures(out, "trajectories", max_failed_fraction)
+    return out

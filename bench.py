@@ -1,0 +1,409 @@
+"""Benchmark of the B200 ensemble integrator (bdsim ChainIntegrator step).
+
+Workload (the reference's headline configuration, seeded synthetic chains):
+  4096 trajectories x N=50 beads, FENE springs b=50, RPY HI h*=0.25 with the
+  Chebyshev square root and Lanczos bounds, Gaussian EV z*=1 d*=0.5, simple
+  shear rate 1, dt=1e-3; initial chains from Gaussian bonds (unit variance),
+  trajectory i seeded with i.
+
+A bench "step" is one chunk of CHUNK=100 integrator steps of every chain (one
+write_every block), i.e. one launch of the persistent integrator kernel. The
+headline value is the FP32-mixed form; the FP64 plain form is measured in the
+same run. `e2e` goes through the reference-facing host-buffer entry point
+(bdcu_integrate_host: pinned R and RNG state copied in, integrated, copied
+out every step).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+For N>1 launch under torch.distributed.run: every rank integrates its own
+shard of 4096 chains (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CHAINS = 4096
+N_BEADS = 50
+CHUNK = 100
+DT = 1e-3
+WORKLOAD = ("4096 chains x N=50, FENE b=50, RPY h*=0.25 Chebyshev+Lanczos, Gauss EV z*=1 d*=0.5, "
+            "shear 1.0, dt=1e-3, gaussian_chain(50, bond_std=1, seed=i), Rng(i)")
+METRIC = "chain-steps/sec at N=50 HI (FP32-mixed vs FP64 plain, 1 B200)"
+# Flop accounting per chain-step (dense-equivalent, the same for both forms):
+#   each D.x product on the 3N-vector counts 2*(3N)^2 flops; each EV pair
+#   evaluation 20 flops (2 evaluations per step, at R and R~); RPY pair
+#   assembly 30 flops per pair (once per step).
+C_EV = 20.0
+C_RPY = 30.0
+
+
+def make_phys():
+    from bdsim_b200.params import DelSMethod, EV, Flow, PhysParams, SimParams, Spring
+    p = PhysParams()
+    p.spring.type = Spring.FENE
+    p.spring.sqrtb = 50.0 ** 0.5
+    p.hstar = 0.25
+    p.hi_method = DelSMethod.Chebyshev
+    p.ev.type = EV.Gauss
+    p.ev.zstar = 1.0
+    p.ev.dstar = 0.5
+    K = np.zeros((3, 3))
+    K[0, 1] = 1.0
+    p.flow = Flow.constant(K)
+    p.number_of_beads = N_BEADS
+    s = SimParams()
+    s.dt = DT
+    return p, s
+
+
+def make_chains(first, count):
+    from bdsim_b200 import initial
+    return [initial.gaussian_chain(N_BEADS, bond_std=1.0, seed=first + i) for i in range(count)]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        loaded = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)  # a 256 MiB write, larger than the 126 MB L2
+
+
+def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream):
+    """Warm up, then time `steps` chunks with CUDA events on the launch stream."""
+    import bdsim_b200 as B
+    from bdsim_b200._abi import CACHE_PERSIST
+    n = len(Rs)
+    with torch.cuda.stream(stream):
+        ens = B.Ensemble([phys] * n, [sim] * n, Rs, [(1, -1, rank_seed0 + i) for i in range(n)], form=form)
+        t = 0.0
+        for _ in range(warmup):
+            ens.advance(t, CHUNK, CACHE_PERSIST)
+            t += CHUNK * DT
+        stream.synchronize()
+        c0 = ens.counter_totals()
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        times = []
+        for _ in range(steps):
+            flush_l2(torch, flush)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ens.advance(t, CHUNK, CACHE_PERSIST)
+            e1.record(stream)
+            t += CHUNK * DT
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        stream.synchronize()
+        c1 = ens.counter_totals()
+        failed = int(ens.failed().sum())
+    delta = {k: c1[k] - c0[k] for k in c1}
+    return {"ms": times, "counters": delta, "failed": failed}
+
+
+def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
+    """Through the host-buffer entry point: pinned R/RNG in, integrate one
+    chunk (a cold spectral cache per call, as a reference integrate call),
+    R/RNG/status out -- every step."""
+    from bdsim_b200 import _abi
+    from bdsim_b200.engine import Context, form_code
+    n = len(Rs)
+    ctx = Context(torch.cuda.current_device())
+    s = type(sim)()
+    s.dt = sim.dt
+    s.implicit_loop_tol = sim.implicit_loop_tol
+    s.time_start = 0.0
+    s.time_end = (CHUNK - 1) * DT
+    ctx.set_chains([phys] * n, [s] * n, [N_BEADS] * n)
+    R = torch.from_numpy(np.concatenate(Rs)).pin_memory()
+    rng = torch.tensor([(1, -1, seed0 + i) for i in range(n)], dtype=torch.int32).pin_memory()
+    status = torch.zeros(n, dtype=torch.int32).pin_memory()
+    Rp, rp, sp = (ctypes.cast(ctypes.c_void_p(x.data_ptr()), tp) for x, tp in
+                  ((R, _abi.c_double_p), (rng, _abi.c_int32_p), (status, _abi.c_int32_p)))
+    ctx.use_stream()
+    fc = form_code(form)
+
+    def once():
+        rc = ctx.lib.bdcu_integrate_host(ctx.h, Rp, rp, sp, None, fc)
+        if rc:
+            raise RuntimeError(ctx.lib.bdcu_last_error(ctx.h).decode())
+
+    for _ in range(warmup):
+        once()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        once()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    h2d = R.numel() * 8 + rng.numel() * 4 + n * (8 + 4)
+    d2h = R.numel() * 8 + rng.numel() * 4 + n * 4
+    return n * CHUNK * steps / wall, h2d, d2h
+
+
+def cpu_reference(seconds_target=15.0, threads=None):
+    """The reference C++ step (oracle/_ref, compiled from the reference
+    sources; the C restatement when that library is absent) on the host
+    cores, on a bounded sample of the workload."""
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    orc = O.ref() if kind == "reference" else O.port()
+    threads = threads or (os.cpu_count() or 1)
+    phys, sim = make_phys()
+    # calibrate on one chain
+    R1 = make_chains(0, 1)
+    s = type(sim)()
+    s.dt, s.time_start, s.time_end = DT, 0.0, 19 * DT
+    t0 = time.perf_counter()
+    orc.integrate_many(R1, [phys], [s], [(1, -1, 0)], 1)
+    per_step = (time.perf_counter() - t0) / 20.0
+    steps = CHUNK
+    chains = max(threads, int(seconds_target / max(per_step * steps, 1e-9)))
+    chains = int(np.ceil(chains / threads) * threads)
+    chains = min(chains, N_CHAINS)
+    Rs = make_chains(0, chains)
+    s.time_end = (steps - 1) * DT
+    t0 = time.perf_counter()
+    _, _, status = orc.integrate_many(Rs, [phys] * chains, [s] * chains, [(1, -1, i) for i in range(chains)], threads)
+    wall = time.perf_counter() - t0
+    return {"value": chains * steps / wall, "unit": "chain-steps/s", "cores": threads, "kind": kind,
+            "sample": f"{chains} of the {N_CHAINS} chains x {steps} steps (one chunk, cold Lanczos start), "
+                      f"{threads} threads, {wall:.1f} s wall"}
+
+
+def flops_per_chain_step(counters):
+    n = 3 * N_BEADS
+    steps = max(counters["steps"], 1)
+    dx = counters["dx_products"] / steps
+    pairs = N_BEADS * (N_BEADS - 1) / 2
+    return dx * 2.0 * n * n + 2 * pairs * C_EV + pairs * C_RPY, dx
+
+
+def measure_peak(fp64):
+    path = os.path.join(ROOT, "bdsim_b200", "libbdsim_peak.so")
+    lib = ctypes.CDLL(path)
+    lib.bdpk_fma_tflops.restype = ctypes.c_double
+    lib.bdpk_fma_tflops.argtypes = [ctypes.c_int, ctypes.c_int]
+    return max(lib.bdpk_fma_tflops(int(fp64), 200000) for _ in range(3))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg (profiling runs)")
+    ap.add_argument("--chains", type=int, default=N_CHAINS, help="chains per GPU (profiling runs use fewer)")
+    ap.add_argument("--forms", default="plain,mixed", help="integrator forms to time")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps, warmup = args.steps, args.warmup
+        vals = []
+        base = None
+        for i in range(warmup + steps):
+            r = cpu_reference(seconds_target=8.0)
+            if i >= warmup:
+                vals.append(r["value"])
+                base = r
+        v = float(np.median(vals))
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "chain-steps/s", "n_gpus": args.gpus,
+                "steps": steps, "warmup": warmup, "ms_per_step": N_CHAINS * CHUNK / v * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": WORKLOAD, "chunk_steps": CHUNK, "n_chains": N_CHAINS},
+                "cpu_baseline": {"value": v, "unit": "chain-steps/s", "cores": base["cores"], "kind": base["kind"],
+                                 "sample": base["sample"]},
+                "e2e": {"value": v, "unit": "chain-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    phys, sim = make_phys()
+    n_chains = args.chains
+    Rs = make_chains(rank * n_chains, n_chains)
+    stream = torch.cuda.Stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    results = {}
+    clocks = None
+    forms = [f for f in args.forms.split(",") if f]
+    for form in forms:
+        barrier()
+        sampler = ClockSampler(local) if form == "mixed" else None
+        if sampler:
+            sampler.start()
+        r = run_form(torch, form, Rs, phys, sim, args.steps, args.warmup, rank * n_chains, stream)
+        if sampler:
+            clocks = sampler.stop()
+        barrier()
+        tot = sum(r["ms"])
+        if dist is not None:
+            t = torch.tensor([tot], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        r["total_ms"] = tot
+        results[form] = r
+
+    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), 1, rank * n_chains,
+                                           "mixed")
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    def rate(r):
+        return world * n_chains * CHUNK * args.steps / (r["total_ms"] * 1e-3)
+
+    if set(forms) != {"plain", "mixed"}:
+        # profiling run: one line per form, no headline
+        for f in forms:
+            print(json.dumps({"form": f, "chain_steps_per_s": rate(results[f]), "ms": results[f]["ms"],
+                              "counters": results[f]["counters"]}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    mixed, plain = results["mixed"], results["plain"]
+    fl_m, dx_m = flops_per_chain_step(mixed["counters"])
+    fl_p, dx_p = flops_per_chain_step(plain["counters"])
+    launch_ms = float(np.mean(mixed["ms"]))
+    peak32 = measure_peak(False)
+    peak64 = measure_peak(True)
+    achieved = n_chains * CHUNK * fl_m / (launch_ms * 1e-3) / 1e12
+    achieved_p = n_chains * CHUNK * fl_p / (float(np.mean(plain["ms"])) * 1e-3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get("mixed_bytes_per_launch")
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cpu = cpu_reference()
+        except Exception as exc:  # reported, not fatal
+            cpu = {"error": str(exc)}
+    line = {
+        "metric": METRIC,
+        "value": rate(mixed),
+        "unit": "chain-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mixed["total_ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64 (mixed)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": "mixed", "chunk_steps": CHUNK, "n_chains_per_gpu": n_chains,
+                   "n_beads": N_BEADS, "l2": "flushed (256 MiB write) between timed chunks",
+                   "parallelism": f"trajectory shards x{world}"},
+        "plain_fp64": {"value": rate(plain), "unit": "chain-steps/s", "ms_per_step": plain["total_ms"] / args.steps,
+                       "dx_per_step": dx_p, "tflops_dense_equiv": achieved_p,
+                       "fp64_frac_of_measured_fma_peak": achieved_p / peak64},
+        "mixed_over_plain": rate(mixed) / rate(plain),
+        "roofline": {"bound": "fp32-simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                     "frac": achieved / peak32, "traffic": traffic,
+                     "peak_source": "measured in this run: FP32 FMA-loop kernel (libbdsim_peak.so); the kernel "
+                                    "runs on CUDA cores, neither HBM- nor tensor-bound",
+                     "flops_per_chain_step": fl_m, "dx_per_step": dx_m,
+                     "hbm_peak_gbs_measured": _peaks().get("hbm_gbs")},
+        "e2e": None if e2e is None else {
+            "value": e2e[0], "unit": "chain-steps/s", "h2d_bytes_per_step": e2e[1], "d2h_bytes_per_step": e2e[2],
+            "path": "bdcu_integrate_host, pinned host R/RNG, cold spectral cache per call"},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "failed_chains": {"mixed": mixed["failed"], "plain": plain["failed"]},
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -6,7 +6,9 @@
                       each with its source file:line.
   ref_steps.npz       outputs of the reference C++ core (oracle/_ref, compiled
                       from the reference sources) for seeded integrations of
-                      every configuration family the integrator supports.
+                      every configuration family the integrator supports:
+                      one multi-step call per case, and the same span taken
+                      one step per call (per-step states, RNG states, times).
 
 Run here, where the reference sources exist:  python tests/golden/make_golden.py
 The GPU tests read only these files, never the reference tree.
@@ -23,6 +25,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from bdsim_b200._abi import count_steps  # noqa: E402
+from bdsim_b200.params import SimParams  # noqa: E402
 from tests.golden.cases import CASES, build_case  # noqa: E402
 
 KNOWN = {
@@ -168,7 +172,27 @@ KNOWN = {
 }
 
 
+def write_singular():
+    """Extract R0_SINGULAR / SINGULAR_HSTAR from the reference's
+    validation/compare_fortran_oracle.py into tests/golden/singular.py."""
+    import re
+    src = open("/root/reference/validation/compare_fortran_oracle.py").read()
+    m = re.search(r"R0_SINGULAR = np\.array\(\[(.*?)\]\)\s*\n\s*SINGULAR_HSTAR = ([0-9.eE+-]+)", src, re.S)
+    rows = re.findall(r"\[([^\[\]]+)\]", m.group(1))
+    arr = np.array([[float(v) for v in r.split(",")] for r in rows])
+    with open(os.path.join(HERE, "singular.py"), "w") as f:
+        f.write('"""R0_SINGULAR / SINGULAR_HSTAR of the reference\'s Fortran cross-check\n'
+                '(validation/compare_fortran_oracle.py:76-100 of the bdsim project): a chain\n'
+                'collapsed onto two points whose RPY tensor is not positive definite.\n'
+                'Extracted from that file by tests/golden/make_golden.py."""\nimport numpy as np\n\n')
+        f.write("R0_SINGULAR = np.array([\n")
+        for r in arr:
+            f.write("    [" + ", ".join(repr(float(v)) for v in r) + "],\n")
+        f.write("])\n\nSINGULAR_HSTAR = " + repr(float(m.group(2))) + "\n")
+
+
 def main():
+    write_singular()
     with open(os.path.join(HERE, "known_answers.json"), "w") as fh:
         json.dump(KNOWN, fh, indent=1)
     from oracle import oracle as O
@@ -183,8 +207,41 @@ def main():
         arrays[f"{name}/R1"] = R1
         arrays[f"{name}/rng"] = np.array(st1, dtype=np.int64)
         arrays[f"{name}/status"] = np.array(status)
+        # the same span one reference step at a time: state k at time
+        # t_k = t0 + k*dt -> state k+1 (each call a fresh model, cold cache)
+        n = count_steps(sim)
+        Rk, st = R0.copy(), (1, -1, seed)
+        Rs, sts, ts = [Rk], [st], []
+        for k in range(n):
+            one = SimParams()
+            one.dt, one.implicit_loop_tol = sim.dt, sim.implicit_loop_tol
+            one.update_center_of_mass = sim.update_center_of_mass
+            one.time_start = one.time_end = sim.time_start + k * sim.dt
+            Rk, st, stt = ref.integrate(Rk, phys, one, st)
+            assert stt == 0
+            Rs.append(Rk)
+            sts.append(st)
+            ts.append(one.time_start)
+        arrays[f"{name}/steps/R"] = np.stack(Rs)
+        arrays[f"{name}/steps/rng"] = np.array(sts, dtype=np.int64)
+        arrays[f"{name}/steps/t"] = np.array(ts)
     np.savez_compressed(os.path.join(HERE, "ref_steps.npz"), **arrays)
     print(f"wrote {len(CASES)} reference cases")
+    # the reference's initial-configuration generators (python/bdsim/initial.py),
+    # loaded by path: they need only numpy
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bdsim_ref_initial",
+                                                  "/root/reference/python/bdsim/initial.py")
+    ri = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ri)
+    init = {}
+    for seed in range(5):
+        init[f"gaussian_chain/{seed}"] = ri.gaussian_chain(17, seed=seed)
+        init[f"fene_fraenkel_chain/{seed}"] = ri.fene_fraenkel_chain(13, 1.0, 2.0, seed=seed)
+        init[f"fene_fraenkel_chain_aligned_x/{seed}"] = ri.fene_fraenkel_chain_aligned_x(9, 1.0, 0.5, seed=seed)
+        init[f"fene_fraenkel_bending_chain/{seed}"] = ri.fene_fraenkel_bending_chain(15, 1.0, 0.1, 5.0, seed=seed)
+    np.savez_compressed(os.path.join(HERE, "initial_chains.npz"), **init)
+    print(f"wrote {len(init)} initial chains")
 
 
 if __name__ == "__main__":
