@@ -240,9 +240,11 @@ def load_library():
     lib.bdcu_total_force.argtypes = [vp, vp, vp]
     lib.bdcu_forces.argtypes = [vp, vp, ctypes.c_double, ctypes.c_int, vp]
     lib.bdcu_ran1.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]
+    lib.bdcu_run_static.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim), c_double_p,
+                                    ctypes.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
     for name in ("bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
                  "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
-                 "bdcu_forces", "bdcu_ran1"):
+                 "bdcu_forces", "bdcu_ran1", "bdcu_run_static"):
         getattr(lib, name).restype = ctypes.c_int
     _LIB = lib
     return lib
@@ -252,7 +254,7 @@ def load_library():
 EXPORTED_SYMBOLS = [
     "bdcu_version", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_last_error",
     "bdcu_set_chains", "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host",
-    "bdcu_total_force", "bdcu_forces", "bdcu_ran1",
+    "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_run_static",
 ]
 
 F_SPRING, F_EV, F_BEND, F_EXTERNAL = 1, 2, 4, 8

@@ -25,37 +25,7 @@ cudaError_t launch_ran1(int n_chains, int32_t* rng, int n_per, double* out, cuda
 
 using namespace bdcu;
 
-struct bdcu_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    int n_chains = 0;
-    int n_max = 0;  // largest 3N
-    int64_t total_beads = 0;
-    int any_hi = 0, any_cheb = 0, need_chol = 0;
-    std::vector<DevChain> chains_h;
-    std::vector<bdcu_sim> sims_h;
-    DevChain* chains_d = nullptr;
-    double* arena_d = nullptr;
-    double* seed_d = nullptr;
-    int seed_len = 0;
-    int32_t* work_d = nullptr;
-    double* scratch_d = nullptr;
-    size_t scratch_bytes = 0;
-    int sm_count = 148;
-    size_t max_smem = 0;
-    // buffers of bdcu_integrate_host
-    double* hR = nullptr;
-    int32_t* hrng = nullptr;
-    double* hcache = nullptr;
-    int32_t* hvalid = nullptr;
-    double* ht0 = nullptr;
-    int32_t* hsteps = nullptr;
-    int32_t* hstatus = nullptr;
-    bdcu_counters* hcnt = nullptr;
-    int64_t hcap_beads = 0;
-    int hcap_chains = 0;
-};
+#include "ctx.h"
 
 namespace {
 
@@ -432,3 +402,8 @@ int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double
 }
 
 }  // extern "C"
+
+namespace bdcu {
+// The per-chain record derivation, for the static-scratch entry point.
+DevChain derive_record(const bdcu_phys& p, const bdcu_sim& s, int64_t bead_off) { return derive(p, s, bead_off); }
+}  // namespace bdcu

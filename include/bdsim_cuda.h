@@ -225,6 +225,32 @@ int bdcu_forces(bdcu_ctx* ctx, const double* R, double t, int which, double* F);
    int32, advanced in place) into out (device, n_chains*n_per_chain). */
 int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double* out);
 
+/* bdcu_run for callers that cannot allocate device memory. No counterpart in
+   the reference: bdsim runs on the CPU and never allocates GPU memory.
+   Some callers cannot call cudaMalloc -- a host application whose memory pool
+   already owns the GPU's memory, or a serving loop that must not take the
+   implicit device-wide synchronisation cudaMalloc/cudaFree imply. This entry
+   point takes the parameters on the host (as bdcu_set_chains does) and runs
+   the same integrator kernel as bdcu_run on the caller's device buffers; the
+   parameter records, arena, work counter and per-block scratch live in one
+   file-scope device array of BDCU_STATIC_SCRATCH_BYTES that every GPU using
+   the library holds until process exit. It calls no cudaMalloc/cudaFree.
+   ctx comes from bdcu_create (which allocates no device memory) and supplies
+   the device, the stream and bdcu_last_error; bdcu_set_chains is not used.
+   - Batches whose parameters plus one block's scratch exceed the array return
+     BDCU_E_LIMIT with a message; smaller batches run with as many concurrent
+     blocks as fit (fewer than bdcu_run may use).
+   - The first call on a device takes the array's device address
+     (cudaGetSymbolAddress): make it before any stream capture on that device.
+   - Every call shares the array and leaves its contents behind; the work
+     counter is cleared by each call. Calls that overlap on the GPU race on the
+     array: serialise them. */
+#define BDCU_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bdcu_sim* sim,
+                    const double* arena, int64_t arena_len, double* R, int32_t* rng, double* cache,
+                    int32_t* cache_valid, const double* t_start, const int32_t* n_steps, int32_t* status,
+                    bdcu_counters* counters, int form, int cache_mode);
+
 #ifdef __cplusplus
 }
 #endif
