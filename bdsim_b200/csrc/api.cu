@@ -12,12 +12,15 @@
 
 #include "bdcu_internal.h"
 #include "integrator.cuh"
+#include "warp_layout.h"
 
 namespace bdcu {
 cudaError_t launch_plain(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t launch_mixed(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t occupancy_plain(int block, size_t smem, int* per_sm);
 cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm);
+cudaError_t launch_mixed_warp(const RunArgs& a, int grid, size_t smem, cudaStream_t s);
+cudaError_t occupancy_mixed_warp(size_t smem, int* per_sm);
 cudaError_t launch_forces(const DevChain* chains, int n_chains, int n_max, const double* arena, const double* R,
                           double t, int which, double* F, cudaStream_t s);
 cudaError_t launch_ran1(int n_chains, int32_t* rng, int n_per, double* out, cudaStream_t s);
@@ -162,6 +165,53 @@ int plan_launch(bdcu_ctx* ctx, int form, LaunchPlan* pl) {
     return BDCU_OK;
 }
 
+// The FP32-mixed form for batches of chains with N <= 64 (no Cholesky-method
+// chains): one chain per warp (integrator_warp.cuh).
+int run_mixed_warp(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache, int32_t* cache_valid,
+                   const double* t_start, const int32_t* n_steps, int32_t* status, bdcu_counters* counters,
+                   int cache_mode) {
+    const size_t smem = (size_t)warp_smem_bytes(ctx->n_max);
+    if (smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "warp kernel shared memory exceeds the device limit");
+    int per_sm = 0;
+    cudaError_t e = occupancy_mixed_warp(smem, &per_sm);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "occupancy_mixed_warp");
+    if (per_sm < 1) per_sm = 1;
+    const int blocks_needed = (ctx->n_chains + kWarpsPerCta - 1) / kWarpsPerCta;
+    const int grid = std::max(1, std::min(blocks_needed, per_sm * ctx->sm_count));
+    const int64_t stride = ctx->any_hi ? warp_scratch_doubles(ctx->n_max) : 1;
+    const size_t sdoubles = (size_t)stride * grid * kWarpsPerCta;
+    int rc = ensure(ctx, &ctx->scratch_d, sdoubles, &ctx->scratch_bytes);
+    if (rc) return rc;
+    RunArgs a;
+    memset(&a, 0, sizeof(a));
+    a.chains = ctx->chains_d;
+    a.n_chains = ctx->n_chains;
+    a.n_max = ctx->n_max;
+    a.arena = ctx->arena_d;
+    a.seed_table = ctx->seed_d;
+    a.R = R;
+    a.rng = rng;
+    a.cache = cache;
+    a.cache_valid = cache_valid;
+    a.t_start = t_start;
+    a.n_steps = n_steps;
+    a.status = status;
+    a.counters = counters;
+    a.cache_mode = cache_mode;
+    a.need_chol = ctx->need_chol;
+    a.need_d = ctx->any_hi;
+    a.need_lz = ctx->any_cheb;
+    a.work_counter = ctx->work_d;
+    a.scratch = ctx->scratch_d;
+    a.scratch_stride = stride;
+    a.xs_pow = ctx->xs_pow_d;
+    a.a_pow = ctx->a_pow_d;
+    CK(cudaMemsetAsync(ctx->work_d, 0, sizeof(int32_t), ctx->stream));
+    e = launch_mixed_warp(a, grid, smem, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "integrate_warp_kernel launch");
+    return BDCU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -191,7 +241,8 @@ int bdcu_destroy(bdcu_ctx* ctx) {
     if (!ctx) return BDCU_OK;
     cudaSetDevice(ctx->device);
     void* ptrs[] = {ctx->chains_d, ctx->arena_d, ctx->seed_d, ctx->work_d, ctx->scratch_d, ctx->hR, ctx->hrng,
-                    ctx->hcache, ctx->hvalid, ctx->ht0, ctx->hsteps, ctx->hstatus, ctx->hcnt};
+                    ctx->hcache, ctx->hvalid, ctx->ht0, ctx->hsteps, ctx->hstatus, ctx->hcnt, ctx->xs_pow_d,
+                    ctx->a_pow_d};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete ctx;
@@ -225,7 +276,7 @@ int bdcu_set_chains(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bd
     ctx->chains_h.resize(n_chains);
     ctx->sims_h.assign(sim, sim + n_chains);
     int64_t off = 0;
-    int n_max = 0, any_hi = 0, any_cheb = 0, need_chol = 0;
+    int n_max = 0, any_hi = 0, any_cheb = 0, need_chol = 0, any_chol_method = 0;
     for (int i = 0; i < n_chains; ++i) {
         const bdcu_phys& p = phys[i];
         if (p.n_beads < 2 || p.n_beads > kMaxBeads)
@@ -255,9 +306,11 @@ int bdcu_set_chains(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bd
             any_hi = 1;
             need_chol = 1;  // Cholesky method, or the Chebyshev fallback
             if (p.hi_method == BDCU_HI_CHEBYSHEV) any_cheb = 1;
+            if (p.hi_method == BDCU_HI_CHOLESKY) any_chol_method = 1;
         }
     }
     ctx->n_chains = n_chains;
+    ctx->any_chol_method = any_chol_method;
     ctx->n_max = n_max;
     ctx->total_beads = off;
     ctx->any_hi = any_hi;
@@ -278,6 +331,29 @@ int bdcu_set_chains(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bd
     }
     if (!ctx->work_d)
         if ((rc = ensure(ctx, &ctx->work_d, 1))) return rc;
+    if (!ctx->xs_pow_d) {
+        // RNG jump-ahead tables: columns of M^k for the xorshift step M
+        // (ux ^= ux<<13; ux ^= ux>>17; ux ^= ux<<5, linear over GF(2)) and
+        // 16807^k mod (2^31-1), k = 0..kMaxDraws
+        std::vector<uint32_t> cols((size_t)(kMaxDraws + 1) * 32);
+        std::vector<uint32_t> apow(kMaxDraws + 1);
+        for (int i = 0; i < 32; ++i) cols[i] = 1u << i;
+        apow[0] = 1;
+        for (int k = 1; k <= kMaxDraws; ++k) {
+            for (int i = 0; i < 32; ++i) {
+                uint32_t u = cols[(size_t)(k - 1) * 32 + i];
+                u ^= (u << 13);
+                u ^= (u >> 17);
+                u ^= (u << 5);
+                cols[(size_t)k * 32 + i] = u;
+            }
+            apow[k] = (uint32_t)(((uint64_t)apow[k - 1] * 16807ull) % 2147483647ull);
+        }
+        if ((rc = ensure(ctx, &ctx->xs_pow_d, cols.size()))) return rc;
+        if ((rc = ensure(ctx, &ctx->a_pow_d, apow.size()))) return rc;
+        CK(cudaMemcpy(ctx->xs_pow_d, cols.data(), sizeof(uint32_t) * cols.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->a_pow_d, apow.data(), sizeof(uint32_t) * apow.size(), cudaMemcpyHostToDevice));
+    }
     return BDCU_OK;
 }
 
@@ -289,6 +365,8 @@ int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache, int32_t* cac
         return fail(ctx, BDCU_E_ARG, "null device pointer");
     if (form != BDCU_FORM_PLAIN_FP64 && form != BDCU_FORM_MIXED_FP32) return fail(ctx, BDCU_E_ARG, "unknown form");
     CK(cudaSetDevice(ctx->device));
+    if (form == BDCU_FORM_MIXED_FP32 && ctx->n_max <= kWarpMaxn && !ctx->any_chol_method)
+        return run_mixed_warp(ctx, R, rng, cache, cache_valid, t_start, n_steps, status, counters, cache_mode);
     LaunchPlan pl;
     int rc = plan_launch(ctx, form, &pl);
     if (rc) return rc;
@@ -318,6 +396,8 @@ int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache, int32_t* cac
     a.work_counter = ctx->work_d;
     a.scratch = ctx->scratch_d;
     a.scratch_stride = std::max<int64_t>(pl.scl.total, 1);
+    a.xs_pow = ctx->xs_pow_d;
+    a.a_pow = ctx->a_pow_d;
     CK(cudaMemsetAsync(ctx->work_d, 0, sizeof(int32_t), ctx->stream));
     cudaError_t e = (form == BDCU_FORM_MIXED_FP32) ? launch_mixed(a, pl.grid, pl.block, pl.smem, ctx->stream)
                                                    : launch_plain(a, pl.grid, pl.block, pl.smem, ctx->stream);

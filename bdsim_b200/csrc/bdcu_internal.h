@@ -70,8 +70,12 @@ struct RunArgs {
     int32_t need_d;         // some chain has HI (dense D in the plain form)
     int32_t need_lz;        // some chain uses the Chebyshev method (Lanczos)
     int32_t* work_counter;  // persistent-grid chain queue (zeroed before launch)
-    double* scratch;        // per-CTA global scratch
-    int64_t scratch_stride; // doubles per CTA
+    double* scratch;        // per-CTA (per-warp for the warp kernel) global scratch
+    int64_t scratch_stride; // doubles per CTA (per warp)
+    const uint32_t* xs_pow; // xorshift step matrix powers: columns of M^k, 32 words per k
+    const uint32_t* a_pow;  // 16807^k mod (2^31 - 1)
 };
+
+constexpr int kMaxDraws = 3 * kMaxBeads;  // jump-ahead tables cover k = 0..kMaxDraws
 
 }  // namespace bdcu

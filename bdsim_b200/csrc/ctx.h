@@ -18,7 +18,9 @@ struct bdcu_ctx {
     int n_chains = 0;
     int n_max = 0;  // largest 3N
     int64_t total_beads = 0;
-    int any_hi = 0, any_cheb = 0, need_chol = 0;
+    int any_hi = 0, any_cheb = 0, need_chol = 0, any_chol_method = 0;
+    uint32_t* xs_pow_d = nullptr;  // RNG jump-ahead tables (uploaded once)
+    uint32_t* a_pow_d = nullptr;
     std::vector<DevChain> chains_h;
     std::vector<bdcu_sim> sims_h;
     DevChain* chains_d = nullptr;

@@ -1,0 +1,947 @@
+// integrator_warp.cuh -- the FP32-mixed form with one chain per WARP, for
+// chains of up to 64 beads. Each warp claims chains from the device work
+// queue and owns one chain at a time; lane l owns beads l and l+32, holding
+// their positions, forces and noise in registers. There is no block-wide
+// barrier: neighbour data (bonds, prefix sums) goes through the warp's own
+// shared-memory area under __syncwarp, reductions are warp shuffles.
+//
+// Precision (the mixed form): D.x recomputed pairwise in FP32 from shared FP32
+// bead coordinates, FP32 excluded volume and Chebyshev recurrence; FP64
+// positions, spring/bending forces, connector solve, Lanczos vectors and
+// tridiagonal bounds, and the (rare) Cholesky fallback. The noise stream is
+// the reference's ran_1 stream bit for bit, drawn by 32 lanes at once with a
+// jump-ahead (GF(2) powers of the xorshift step, powers of 16807 mod 2^31-1).
+//
+// Reference: src/integrator.cpp:61-170 of the bdsim project and the physics it
+// calls; each stage cites its reference function.
+#pragma once
+
+#include "integrator.cuh"
+#include "warp_layout.h"
+
+namespace bdcu {
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Number of eigenvalues of the tridiagonal (a, b) below x, from the signs of
+// the leading principal minors p_i = (a_i - x) p_{i-1} - b_{i-1}^2 p_{i-2}
+// (divide-free Sturm sequence, rescaled against overflow). The mixed form
+// uses it in place of sturm_count (src/hydrodynamics.cpp:91-104).
+__device__ __forceinline__ int sturm_count_products(const double* a, const double* b, int m, double x) {
+    double pm = 1.0, p = a[0] - x;
+    int count = (p < 0.0) ? 1 : 0;
+    for (int i = 1; i < m; ++i) {
+        const double pn = (a[i] - x) * p - b[i - 1] * b[i - 1] * pm;
+        count += ((pn < 0.0) != (p < 0.0)) ? 1 : 0;
+        pm = p;
+        p = pn;
+        if (fabs(p) > 1e150) {
+            p *= 1e-150;
+            pm *= 1e-150;
+        }
+    }
+    return count;
+}
+
+// Bisection for the target-th eigenvalue boundary on a half warp (16 lanes,
+// depth-4 speculative tree), the iteration of src/hydrodynamics.cpp:251-260.
+static __device__ void halfwarp_bisect(const double* al, const double* bb, int k, int target, double& lo, double& hi) {
+    const int lane = threadIdx.x & 15;
+    const int lvl = 31 - __clz(lane + 1);
+    const int p = lane + 1 - (1 << lvl);
+    for (int it = 0; it < 100; it += 4) {
+        int dec = 0;
+        if (lane < 15) {
+            double a = lo, b = hi;
+            for (int l = 0; l < lvl; ++l) {
+                const int bit = (p >> (lvl - 1 - l)) & 1;
+                const double m = 0.5 * (a + b);
+                if (bit == 0) b = m; else a = m;
+            }
+            const double mid = 0.5 * (a + b);
+            dec = (sturm_count_products(al, bb, k, mid) >= target) ? 0 : 1;
+        }
+        int node = 0;
+        double na = lo, nb = hi;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int d = __shfl_sync(kFull, dec, node, 16);
+            const double m = 0.5 * (na + nb);
+            if (d == 0) nb = m; else na = m;
+            node = 2 * node + 1 + d;
+        }
+        const bool same = (na == lo && nb == hi);
+        lo = na;
+        hi = nb;
+        // both half warps keep iterating until both are settled
+        if (__all_sync(kFull, same)) break;
+    }
+}
+
+// Inverse iteration for a Ritz vector (src/hydrodynamics.cpp:106-136), one lane.
+static __device__ void wk_tridiag_vec(const double* a, const double* b, int m, double lambda, double* y) {
+    const double scale = dmax_(fabs(lambda), 1.0);
+    const double shift = lambda - 1.0e-7 * scale;
+    double c[kLanczosCold], d[kLanczosCold];
+    const double y0 = rsqrt((double)m);
+    for (int i = 0; i < m; ++i) y[i] = y0;
+    for (int it = 0; it < 2; ++it) {
+        double beta0 = a[0] - shift;
+        if (fabs(beta0) < 1.0e-300) beta0 = 1.0e-300;
+        double ib = 1.0 / beta0;
+        c[0] = (m > 1 ? b[0] * ib : 0.0);
+        d[0] = y[0] * ib;
+        for (int i = 1; i < m; ++i) {
+            double beta = (a[i] - shift) - b[i - 1] * c[i - 1];
+            if (fabs(beta) < 1.0e-300) beta = 1.0e-300;
+            ib = 1.0 / beta;
+            c[i] = (i < m - 1 ? b[i] * ib : 0.0);
+            d[i] = (y[i] - b[i - 1] * d[i - 1]) * ib;
+        }
+        y[m - 1] = d[m - 1];
+        for (int i = m - 2; i >= 0; --i) y[i] = d[i] - c[i] * y[i + 1];
+        double nrm = 0.0;
+        for (int i = 0; i < m; ++i) nrm += y[i] * y[i];
+        nrm = sqrt(nrm);
+        if (!(nrm > 0.0) || !isfinite(nrm)) {
+            for (int i = 0; i < m; ++i) y[i] = y0;
+            return;
+        }
+        const double inr = 1.0 / nrm;
+        for (int i = 0; i < m; ++i) y[i] *= inr;
+    }
+}
+
+struct WarpChain {
+    const RunArgs& a;
+    WarpShared& S;
+    const DevChain& ch;
+    double* V;      // warm Lanczos basis in shared memory (kLanczosWarm x nv)
+    double* Vg;     // cold basis in global scratch (kLanczosCold x nv)
+    double* Lt;     // Cholesky factor in global scratch (n x n)
+    int nv;
+    int lane;
+    int N, n;
+    bool hi;
+    int64_t cnt[8];
+    int status;
+    // RPY constants (FP32)
+    float hs, TRPIhs, K1, K2, K3, C3ihs, C7ihs;
+
+    __device__ WarpChain(const RunArgs& a_, WarpShared& S_, const DevChain& ch_) : a(a_), S(S_), ch(ch_) {}
+
+    __device__ __forceinline__ bool valid(int q) const { return lane + 32 * q < N; }
+
+    // ---- FP32 matrix-free D.x (Diffusion::apply, src/mobility.cpp:53-56;
+    // RPY weights src/hydrodynamics.cpp:77-105). x, y: the lane's two beads.
+    __device__ void apply(const double (&x)[2][3], double (&y)[2][3]) {
+        if (!hi) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) y[q][d] = x[q][d];
+            return;
+        }
+        cnt[C_DX] += 1;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (valid(q)) S.xs[lane + 32 * q] = make_float4((float)x[q][0], (float)x[q][1], (float)x[q][2], 0.f);
+        __syncwarp();
+        float acc[2][3];
+        float4 pb[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            pb[q] = valid(q) ? S.pos[lane + 32 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) acc[q][d] = (float)x[q][d];
+        }
+        for (int j = 0; j < N; ++j) {
+            const float4 pj = S.pos[j];
+            const float4 xj = S.xs[j];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
+                const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
+                const float rinv = rsqrtf(sq);
+                const float rs = sq * rinv;
+                const float hr = hs * rinv;
+                const float hr2 = hr * hr;
+                const bool far = rs >= TRPIhs;
+                float om1 = far ? hr * (K1 + K2 * hr2) : 1.f - C3ihs * rs;
+                float om2 = far ? hr * rinv * rinv * (K1 - K3 * hr2) : C7ihs * rs * rinv * rinv;
+                const bool self = (j == lane + 32 * q);
+                om1 = self ? 0.f : om1;
+                om2 = self ? 0.f : om2;
+                const float t = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
+                acc[q][0] += om1 * xj.x + t * dx;
+                acc[q][1] += om1 * xj.y + t * dy;
+                acc[q][2] += om1 * xj.z + t * dz;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) y[q][d] = valid(q) ? (double)acc[q][d] : 0.0;
+    }
+
+    __device__ double dot(const double (&x)[2][3], const double (&y)[2][3]) const {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s += x[q][d] * y[q][d];
+        return wsum(s);
+    }
+
+    __device__ void stage_pos(const double (&R)[2][3]) {
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (valid(q)) S.pos[lane + 32 * q] = make_float4((float)R[q][0], (float)R[q][1], (float)R[q][2], 0.f);
+        __syncwarp();
+    }
+
+    __device__ void to_smem(double* buf, const double (&x)[2][3]) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (valid(q))
+#pragma unroll
+                for (int d = 0; d < 3; ++d) buf[3 * (lane + 32 * q) + d] = x[q][d];
+    }
+
+    // ---- forces at R (FP64 springs/bending/external, FP32 EV) ------------
+    // Fs: spring bead forces (src/spring.cpp:195-207). Fe: (EV + bending) +
+    // external(t) (src/model.hpp:56-64). Positions must be staged (S.pos) and
+    // R copied to S.s0.
+    __device__ void forces(const double (&R)[2][3], double t, double (&Fs)[2][3], double (&Fe)[2][3], bool spring) {
+        to_smem(S.s0, R);
+        __syncwarp();
+        // bonds b = lane, lane+32 (b < N-1): Fc -> s1, unit bonds -> s2, lengths -> s3
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int b = lane + 32 * q;
+            if (b < N - 1) {
+                const double b0 = S.s0[3 * b + 3] - S.s0[3 * b], b1 = S.s0[3 * b + 4] - S.s0[3 * b + 1],
+                             b2 = S.s0[3 * b + 5] - S.s0[3 * b + 2];
+                const double len = clamped_len(b0, b1, b2);
+                const double f = connector_factor(ch, len);
+                S.s1[3 * b] = f * b0;
+                S.s1[3 * b + 1] = f * b1;
+                S.s1[3 * b + 2] = f * b2;
+                const double il = 1.0 / len;
+                S.s2[3 * b] = il * b0;
+                S.s2[3 * b + 1] = il * b1;
+                S.s2[3 * b + 2] = il * b2;
+                S.s3[b] = len;
+            }
+        }
+        __syncwarp();
+        const bool bend = ch.bend_type != BDCU_BEND_NONE && N > 2;
+        if (bend) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int b = lane + 32 * q;
+                if (b < N - 2)
+                    S.s4[b] = S.s2[3 * (b + 1)] * S.s2[3 * b] + S.s2[3 * (b + 1) + 1] * S.s2[3 * b + 1] +
+                              S.s2[3 * (b + 1) + 2] * S.s2[3 * b + 2];
+            }
+            __syncwarp();
+        }
+        const float zs = (float)ch.zsbyds5, p5 = (float)ch.pt5bydssq;
+        const double* phi = (ch.ev_type == BDCU_EV_SDK && ch.phi_off >= 0) ? a.arena + ch.phi_off : nullptr;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int m = lane + 32 * q;
+            if (!valid(q)) {
+                for (int d = 0; d < 3; ++d) Fs[q][d] = Fe[q][d] = 0.0;
+                continue;
+            }
+            if (spring) {
+                for (int d = 0; d < 3; ++d) {
+                    double v;
+                    if (m == 0) v = S.s1[d];
+                    else if (m == N - 1) v = -S.s1[3 * (N - 2) + d];
+                    else v = S.s1[3 * m + d] - S.s1[3 * (m - 1) + d];
+                    Fs[q][d] = v;
+                }
+            }
+            // excluded volume, FP32 pair sums: the force on m from j is
+            // -fac(r) (R_j - R_m), |j - m| >= contour distance
+            float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+            if (ch.ev_type != BDCU_EV_NONE) {
+                const float4 pm = S.pos[m];
+                for (int j = 0; j < N; ++j) {
+                    const int dj = j > m ? j - m : m - j;
+                    if (dj < ch.cd || j == m) continue;
+                    const float4 pj = S.pos[j];
+                    const float dx = pj.x - pm.x, dy = pj.y - pm.y, dz = pj.z - pm.z;
+                    const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
+                    float fac;
+                    if (ch.ev_type == BDCU_EV_GAUSS) {
+                        fac = zs * __expf(-sq * p5);
+                    } else {
+                        const int mu = j < m ? j : m, nu = j < m ? m : j;
+                        fac = (float)ev_factor(ch, sqrt((double)sq), phi ? phi[mu * N + nu] : 0.0);
+                    }
+                    f0 -= fac * dx;
+                    f1 -= fac * dy;
+                    f2 -= fac * dz;
+                }
+            }
+            double fb[3] = {0.0, 0.0, 0.0}, fx[3] = {0.0, 0.0, 0.0};
+            if (bend) bending_on_bead(ch, m, S.s2, S.s4, S.s3, fb);
+            if (ch.ext_n > 0) external_on_bead(ch, a.arena, m, t, fx);
+            Fe[q][0] = ((double)f0 + fb[0]) + fx[0];
+            Fe[q][1] = ((double)f1 + fb[1]) + fx[1];
+            Fe[q][2] = ((double)f2 + fb[2]) + fx[2];
+        }
+        __syncwarp();
+    }
+
+    // ---- noise: the 3N draws of raw_noise (src/mobility.cpp:18-29) -------
+    // 32 lanes draw contiguous blocks of the stream; lane l jumps to draw l*c
+    // with the tabulated powers, so the uniforms equal ran_1's, bit for bit.
+    __device__ void noise(uint32_t& ux0, int32_t& iy0, int32_t& seed, double (&X)[2][3]) {
+        if (seed <= 0 || iy0 < 0) {
+            const int32_t s = seed < 0 ? -seed : seed;
+            iy0 = (888889999 ^ s) | 1;
+            ux0 = (uint32_t)(777755555 ^ s);
+            seed = s + 1;
+        }
+        const int c = (n + 31) / 32;
+        const int k0 = lane * c;
+        const int k1 = min(n, k0 + c);
+        uint32_t ux = 0;
+        int32_t iy = 0;
+        if (k0 < n) {
+            const uint32_t* cols = a.xs_pow + 32 * (int64_t)k0;
+#pragma unroll 8
+            for (int i = 0; i < 32; ++i) ux ^= cols[i] & (0u - ((ux0 >> i) & 1u));
+            iy = (int32_t)(((uint64_t)a.a_pow[k0] * (uint64_t)(uint32_t)iy0) % 2147483647ull);
+            const float am = __fdiv_rn(__int_as_float(0x3f7fffff), 2147483648.0f);
+            for (int k = k0; k < k1; ++k) {
+                ux ^= (ux << 13);
+                ux ^= (ux >> 17);
+                ux ^= (ux << 5);
+                const int32_t kk = iy / 127773;
+                iy = 16807 * (iy - kk * 127773) - 2836 * kk;
+                if (iy < 0) iy += 2147483647;
+                const uint32_t mixed = ux ^ (uint32_t)iy;
+                const int32_t res = (int32_t)((mixed & 0x7fffffffu) | 1u);
+                S.s0[k] = (double)__fmul_rn(am, __int2float_rn(res));
+            }
+        }
+        const int last = (n - 1) / c;
+        ux0 = __shfl_sync(kFull, ux, last);
+        iy0 = __shfl_sync(kFull, iy, last);
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double v = 0.0;
+                if (valid(q)) {
+                    const double y = S.s0[3 * (lane + 32 * q) + d] - 0.5;
+                    v = (14.14855378 * y * y + 1.21569221) * y;
+                }
+                X[q][d] = v;
+            }
+        __syncwarp();
+    }
+
+    // ---- Lanczos extreme eigenvalues (src/hydrodynamics.cpp:146-264) ----
+    __device__ double* basis(int j, int m) { return (m <= kLanczosWarm ? V : Vg) + (int64_t)j * nv; }
+    __device__ void load(const double* vec, double (&x)[2][3]) const {
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) x[q][d] = valid(q) ? vec[3 * (lane + 32 * q) + d] : 0.0;
+    }
+    __device__ void store(double* vec, const double (&x)[2][3]) const {
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (valid(q))
+#pragma unroll
+                for (int d = 0; d < 3; ++d) vec[3 * (lane + 32 * q) + d] = x[q][d];
+    }
+
+    // Returns rmin/rmax; writes the Ritz vectors.
+    __device__ int lanczos(int m, bool warm, const double* cache, double (&vmin)[2][3], double (&vmax)[2][3],
+                           double& rmin, double& rmax) {
+        if (n < m) m = n;
+        double v[2][3], w[2][3], vp[2][3];
+        if (warm) {
+            load(cache, v);
+            double nv2 = sqrt(dot(v, v));
+            if (!(nv2 > 0.0)) {
+                load(a.seed_table, v);
+                nv2 = ch.seed_norm;
+            }
+            const double inv = 1.0 / nv2;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) v[q][d] *= inv;
+        } else {
+            load(a.seed_table, v);
+            const double inv = 1.0 / ch.seed_norm;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) v[q][d] *= inv;
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vp[q][d] = 0.0;
+        int k = 0;
+        double b = 0.0;
+        for (int j = 0; j < m; ++j) {
+            store(basis(j, m), v);
+            apply(v, w);
+            const double al = dot(v, w);
+            if (lane == 0) S.alpha[k] = al;
+            ++k;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) w[q][d] -= al * v[q][d] + b * vp[q][d];
+            __syncwarp();
+            for (int u = 0; u <= j; ++u) {
+                double uu[2][3];
+                load(basis(u, m), uu);
+                const double dd = dot(w, uu);
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) w[q][d] -= dd * uu[q][d];
+            }
+            b = sqrt(dot(w, w));
+            if (b < 1.0e-10) break;
+            const double ib = 1.0 / b;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    vp[q][d] = v[q][d];
+                    v[q][d] = w[q][d] * ib;
+                }
+            if (lane == 0) S.beta[j] = b;
+        }
+        __syncwarp();
+        if (k == 1) {
+            rmin = rmax = S.alpha[0];
+            load(basis(0, m), vmin);
+            load(basis(0, m), vmax);
+            return 1;
+        }
+        double lo = S.alpha[0], hi = S.alpha[0];
+        for (int i = 0; i < k; ++i) {
+            const double rad = (i > 0 ? fabs(S.beta[i - 1]) : 0.0) + (i < k - 1 ? fabs(S.beta[i]) : 0.0);
+            lo = dmin_(lo, S.alpha[i] - rad);
+            hi = dmax_(hi, S.alpha[i] + rad);
+        }
+        // lanes 0-15 bracket the smallest eigenvalue, lanes 16-31 the largest
+        double l2 = lo, h2 = hi;
+        halfwarp_bisect(S.alpha, S.beta, k, lane < 16 ? 1 : k, l2, h2);
+        const double r = 0.5 * (l2 + h2);
+        rmin = __shfl_sync(kFull, r, 0);
+        rmax = __shfl_sync(kFull, r, 16);
+        if (lane == 0) wk_tridiag_vec(S.alpha, S.beta, k, rmin, S.ymin);
+        if (lane == 16) wk_tridiag_vec(S.alpha, S.beta, k, rmax, S.ymax);
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vmin[q][d] = vmax[q][d] = 0.0;
+        for (int j = 0; j < k; ++j) {
+            double vj[2][3];
+            load(basis(j, m), vj);
+            const double y1 = S.ymin[j], y2 = S.ymax[j];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    vmin[q][d] += y1 * vj[q][d];
+                    vmax[q][d] += y2 * vj[q][d];
+                }
+        }
+        __syncwarp();
+        return k;
+    }
+
+    // spectral_bounds (src/hydrodynamics.cpp:224-264): the warm-start vector
+    // lives in the chain's cache slice.
+    __device__ void bounds(double* cache, int& cache_valid, double& lmin, double& lmax) {
+        double vmin[2][3], vmax[2][3], rmin, rmax;
+        const bool can_warm = cache_valid != 0;
+        const int steps = lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, cache, vmin, vmax, rmin, rmax);
+        if (can_warm && steps < 4) {
+            lanczos(kLanczosCold, false, cache, vmin, vmax, rmin, rmax);
+            cnt[C_LZCOLD] += 1;
+        } else {
+            cnt[can_warm ? C_LZWARM : C_LZCOLD] += 1;
+        }
+        double s[2][3], u[2][3];
+        load(a.seed_table, u);
+        const double iun = 1.0 / ch.seed_norm;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s[q][d] = vmin[q][d] + vmax[q][d] + 0.01 * u[q][d] * iun;
+        const double sn = sqrt(dot(s, s));
+        if (sn > 0.0 && isfinite(sn)) {
+            const double is = 1.0 / sn;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) s[q][d] *= is;
+            store(cache, s);
+            cache_valid = 1;
+        } else {
+            cache_valid = 0;
+        }
+        lmin = 0.5 * rmin;
+        lmax = 1.02 * rmax;
+        if (lmin < 1.0e-12) lmin = 1.0e-12;
+        if (lmin >= lmax) lmin = lmax * 1.0e-6;
+    }
+
+    // ---- Chebyshev square root, FP32 recurrence (src/hydrodynamics.cpp:267-337)
+    // Returns the FD error; out = approx D^{1/2} x0.
+    __device__ double chebyshev(const double (&x0)[2][3], double lmin, double lmax, double (&out)[2][3]) {
+        double Dx0[2][3];
+        apply(x0, Dx0);
+        const double x0Dx0 = dot(x0, Dx0);
+        double Lr = sqrt(lmax / lmin) * ch.mult + 0.5;
+        int L = !(Lr < 2.0e9) ? kMaxCheb : (int)Lr + 1;
+        L = L > kMaxCheb ? kMaxCheb : (L < 2 ? 2 : L);
+        const float da = (float)(2.0 / (lmax - lmin));
+        const float db = (float)(-(lmax + lmin) / (lmax - lmin));
+        double fd = 0.0;
+        for (;;) {
+            const float inv = 1.f / (float)(L + 1);
+            for (int k = lane; k <= L; k += 32) {
+                const float xk = cospif(((float)k + 0.5f) * inv) / da - db / da;
+                S.sqx[k] = sqrtf(xk);
+            }
+            __syncwarp();
+            for (int j = lane; j <= L; j += 32) {
+                float s = 0.f;
+                for (int k = 0; k <= L; ++k) s += S.sqx[k] * cospif((float)j * ((float)k + 0.5f) * inv);
+                s *= 2.f * inv;
+                if (j == 0) s *= 0.5f;
+                S.coef[j] = s;
+            }
+            __syncwarp();
+            float tp[2][3], tc[2][3], o[2][3];
+            const float c0 = S.coef[0], c1 = S.coef[1];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    tp[q][d] = (float)x0[q][d];
+                    tc[q][d] = da * (float)Dx0[q][d] + db * tp[q][d];
+                    o[q][d] = c0 * tp[q][d] + c1 * tc[q][d];
+                }
+            for (int l = 2; l <= L; ++l) {
+                double tcd[2][3], Dv[2][3];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) tcd[q][d] = tc[q][d];
+                apply(tcd, Dv);
+                const float cl = S.coef[l];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const float tn = 2.f * (da * (float)Dv[q][d] + db * tc[q][d]) - tp[q][d];
+                        tp[q][d] = tc[q][d];
+                        tc[q][d] = tn;
+                        o[q][d] += cl * tn;
+                    }
+            }
+            cnt[C_CHEB] += L;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) out[q][d] = valid(q) ? (double)o[q][d] : 0.0;
+            const double rr = dot(out, out);
+            fd = fabs(rr - x0Dx0) / x0Dx0;
+            __syncwarp();
+            if (fd <= ch.fd_tol || L >= kMaxCheb) break;
+            const int grow = L / 4 > 1 ? L / 4 : 1;
+            L = (L + grow) > kMaxCheb ? kMaxCheb : L + grow;
+        }
+        return fd;
+    }
+
+    // ---- Cholesky fallback (src/mobility.cpp:69-81): dense FP64 D in global
+    // scratch, right-looking factor, L x0. Returns false if not PD.
+    __device__ bool cholesky_noise(const double (&R)[2][3], const double (&x0)[2][3], double (&out)[2][3]) {
+        to_smem(S.s0, R);
+        __syncwarp();
+        double* L = Lt;
+        for (int idx = lane; idx < 9 * N; idx += 32) {
+            const int mu = idx / 9, i = (idx % 9) / 3, j = idx % 3;
+            L[(int64_t)(3 * mu + i) * n + 3 * mu + j] = (i == j) ? 1.0 : 0.0;
+        }
+        const int npairs = N * (N - 1) / 2;
+        for (int pidx = lane; pidx < npairs; pidx += 32) {
+            int nu = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pidx)) * 0.5);
+            while (nu * (nu - 1) / 2 > pidx) --nu;
+            while ((nu + 1) * nu / 2 <= pidx) ++nu;
+            const int mu = pidx - nu * (nu - 1) / 2;
+            double b[3];
+            for (int d = 0; d < 3; ++d) b[d] = S.s0[3 * nu + d] - S.s0[3 * mu + d];
+            double om1, om2;
+            rpy_weights(ch.hstar, b[0] * b[0] + b[1] * b[1] + b[2] * b[2], om1, om2);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double val = om2 * b[i] * b[j] + (i == j ? om1 : 0.0);
+                    L[(int64_t)(3 * mu + i) * n + 3 * nu + j] = val;
+                    L[(int64_t)(3 * nu + j) * n + 3 * mu + i] = val;
+                }
+        }
+        __syncwarp();
+        for (int k = 0; k < n; ++k) {
+            const double s = L[(int64_t)k * n + k];
+            if (!(s > 0.0)) return false;
+            const double dk = sqrt(s);
+            __syncwarp();
+            if (lane == 0) L[(int64_t)k * n + k] = dk;
+            const double idk = 1.0 / dk;
+            for (int i = k + 1 + lane; i < n; i += 32) L[(int64_t)k * n + i] *= idk;
+            __syncwarp();
+            const double* colk = L + (int64_t)k * n;
+            for (int j = k + 1; j < n; ++j) {
+                const double ljk = colk[j];
+                for (int i = j + lane; i < n; i += 32) L[(int64_t)j * n + i] -= colk[i] * ljk;
+            }
+            __syncwarp();
+        }
+        to_smem(S.s1, x0);
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const int i = 3 * (lane + 32 * q) + d;
+                double s = 0.0;
+                if (valid(q))
+                    for (int j = 0; j <= i; ++j) s += L[(int64_t)j * n + i] * S.s1[j];
+                out[q][d] = s;
+            }
+        __syncwarp();
+        return true;
+    }
+};
+
+// -------------------------------------------------------------- the kernel
+
+__global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const RunArgs a) {
+    extern __shared__ __align__(16) unsigned char wsm[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = warp_smem_stride(a.n_max);
+    WarpShared& S = *reinterpret_cast<WarpShared*>(wsm + stride * warp);
+    double* Vs = reinterpret_cast<double*>(wsm + stride * warp + (sizeof(WarpShared) + 15) / 16 * 16);
+    const int64_t gw = (int64_t)blockIdx.x * kWarpsPerCta + warp;
+    double* scr = a.scratch + gw * a.scratch_stride;
+    const int nvr = (int)round_up8(a.n_max);
+
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(a.work_counter, 1);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= a.n_chains) break;
+        {
+            const int nw = (int)(sizeof(DevChain) / 8);
+            const double* src = reinterpret_cast<const double*>(a.chains + c);
+            double* dst = reinterpret_cast<double*>(&S.ch);
+            for (int i = lane; i < nw; i += 32) dst[i] = src[i];
+        }
+        __syncwarp();
+        const DevChain& ch = S.ch;
+        int status = a.status[c];
+        if ((status & BDCU_ST_FATAL_MASK) || ch.bad_param) {
+            if (lane == 0 && ch.bad_param) a.status[c] = status | BDCU_ST_BAD_PARAM;
+            __syncwarp();
+            continue;
+        }
+        WarpChain W(a, S, ch);
+        W.V = Vs;
+        W.Vg = scr;
+        W.Lt = scr + (int64_t)kLanczosCold * nvr;
+        W.nv = nvr;
+        W.lane = lane;
+        W.N = ch.N;
+        W.n = 3 * ch.N;
+        W.hi = ch.hstar > 0.0;
+        W.status = status;
+        for (int k = 0; k < 8; ++k) W.cnt[k] = 0;
+        {
+            const float RPI = 1.7724538509055160f, TPI = 6.283185307179586f;
+            const float hsf = (float)ch.hstar;
+            W.hs = hsf;
+            W.TRPIhs = 2.f * RPI * hsf;
+            W.K1 = RPI * 0.75f;
+            W.K2 = RPI * 0.75f * (TPI / 3.f);
+            W.K3 = RPI * 0.75f * TPI;
+            W.C3ihs = (0.75f / RPI * 0.375f) / hsf;
+            W.C7ihs = (0.09375f / RPI) / hsf;
+        }
+        const int N = W.N;
+        double* gR = a.R + 3 * ch.bead_off;
+        double* gcache = a.cache + 3 * ch.bead_off;
+        int cache_valid = (a.cache_mode == BDCU_CACHE_PERSIST) ? a.cache_valid[c] : 0;
+        uint32_t ux = (uint32_t)a.rng[3 * c];
+        int32_t iy = a.rng[3 * c + 1], seed = a.rng[3 * c + 2];
+        double R[2][3];
+        W.load(gR, R);
+        const int nsteps = a.n_steps[c];
+        double t = a.t_start[c];
+        const double dt = ch.dt;
+        const double sqrt2inv = 1.0 / sqrt(2.0);
+        const double sqrt_dt = sqrt(dt);
+        for (int step = 0; step < nsteps; ++step) {
+            // recenter (src/integrator.cpp:88-93)
+            if (ch.update_com) {
+                double com[3];
+                for (int d = 0; d < 3; ++d) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) s += R[q][d];
+                    com[d] = (1.0 / N) * wsum(s);
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    if (W.valid(q))
+                        for (int d = 0; d < 3; ++d) R[q][d] -= com[d];
+            }
+            W.stage_pos(R);
+            double Fs[2][3], Fe[2][3];
+            W.forces(R, t, Fs, Fe, true);
+            double X0[2][3], dW[2][3];
+            W.noise(ux, iy, seed, X0);
+            // brownian_step (src/mobility.cpp:58-88)
+            if (!W.hi) {
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) dW[q][d] = sqrt_dt * X0[q][d];
+            } else {
+                double lmin, lmax, bx[2][3];
+                W.bounds(gcache, cache_valid, lmin, lmax);
+                const double fd = W.chebyshev(X0, lmin, lmax, bx);
+                if (!(fd <= ch.fd_tol)) {
+                    W.status |= BDCU_ST_CHEB_FALLBACK;
+                    W.cnt[C_FALLBACK] += 1;
+                    if (!W.cholesky_noise(R, X0, bx)) {
+                        W.status |= BDCU_ST_NOT_PD;
+                        break;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) dW[q][d] = sqrt_dt * bx[q][d];
+            }
+            // predictor (src/integrator.cpp:96-101)
+            double K1[9], K2[9];
+            kappa_at(ch, a.arena, t, K1);
+            kappa_at(ch, a.arena, t + dt, K2);
+            double A[2][3], DF[2][3], Rp[2][3];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) A[q][d] = Fs[q][d] + Fe[q][d];
+            W.apply(A, DF);
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
+                    Rp[q][r] = W.valid(q) ? R[q][r] + dt * (fl1 + 0.25 * DF[q][r]) + sqrt2inv * dW[q][r] : 0.0;
+                }
+            // upsilon (src/integrator.cpp:107-119): forces at R~ with R~'s coordinates staged
+            W.stage_pos(Rp);
+            double Fep[2][3], dummy[2][3];
+            W.forces(Rp, t + dt, dummy, Fep, false);
+            W.stage_pos(R);
+            double DFs[2][3], DFe[2][3], ups[2][3];
+            W.apply(Fs, DFs);
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) A[q][d] = Fe[q][d] + Fep[q][d];
+            W.apply(A, DFe);
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
+                    const double fl2 = K2[3 * r] * Rp[q][0] + K2[3 * r + 1] * Rp[q][1] + K2[3 * r + 2] * Rp[q][2];
+                    ups[q][r] = R[q][r] + dt * (0.5 * (fl1 + fl2) + 0.125 * DFs[q][r] + 0.125 * DFe[q][r]) +
+                                sqrt2inv * dW[q][r];
+                }
+            // solve_connectors (src/integrator.cpp:125-165): lane owns bonds lane, lane+32
+            W.to_smem(S.s0, ups);
+            W.to_smem(S.s1, Rp);
+            __syncwarp();
+            double dups[2][3], bond[2][3];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int b = lane + 32 * q;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const bool ok = b < N - 1;
+                    dups[q][d] = ok ? S.s0[3 * (b + 1) + d] - S.s0[3 * b + d] : 0.0;
+                    bond[q][d] = ok ? S.s1[3 * (b + 1) + d] - S.s1[3 * b + d] : 0.0;
+                }
+            }
+            const double anchor0 = S.s1[0], anchor1 = S.s1[1], anchor2 = S.s1[2];
+            __syncwarp();
+            double Rprev[2][3], Rc[2][3];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Rprev[q][d] = Rp[q][d];
+            const int max_iter = 100 * N;
+            const double c8 = 0.125 * dt, c4 = 0.25 * dt;
+            int lstat = 0;
+            for (int iter = 0;; ++iter) {
+                // connector forces (src/spring.cpp:234-244) into s1, bead forces
+                double Fc[2][3];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int b = lane + 32 * q;
+                    const double f =
+                        b < N - 1 ? connector_factor(ch, clamped_len(bond[q][0], bond[q][1], bond[q][2])) : 0.0;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        Fc[q][d] = f * bond[q][d];
+                        if (b < N - 1) S.s1[3 * b + d] = Fc[q][d];
+                    }
+                }
+                __syncwarp();
+                double Fb[2][3], DFb[2][3];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int m = lane + 32 * q;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        double v = 0.0;
+                        if (m < N) {
+                            if (m == 0) v = S.s1[d];
+                            else if (m == N - 1) v = -S.s1[3 * (N - 2) + d];
+                            else v = S.s1[3 * m + d] - S.s1[3 * (m - 1) + d];
+                        }
+                        Fb[q][d] = v;
+                    }
+                }
+                __syncwarp();
+                W.apply(Fb, DFb);
+                W.to_smem(S.s2, DFb);
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int b = lane + 32 * q;
+                    if (b < N - 1) {
+                        double g[3], qv[3];
+                        for (int d = 0; d < 3; ++d)
+                            g[d] = dups[q][d] + c8 * (S.s2[3 * (b + 1) + d] - S.s2[3 * b + d]) + c4 * Fc[q][d];
+                        solve_connector(g, dt, ch, qv, lstat);
+                        for (int d = 0; d < 3; ++d) bond[q][d] = qv[d];
+                    }
+                }
+                // R_corr = anchor + prefix sums of the bonds (warp scan, two segments)
+                double scan[2][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double v0 = bond[0][d], v1 = bond[1][d];
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const double t0 = __shfl_up_sync(kFull, v0, o);
+                        const double t1 = __shfl_up_sync(kFull, v1, o);
+                        if (lane >= o) {
+                            v0 += t0;
+                            v1 += t1;
+                        }
+                    }
+                    const double carry = __shfl_sync(kFull, v0, 31);
+                    scan[0][d] = v0;
+                    scan[1][d] = v1 + carry;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    S.s1[0] = anchor0;
+                    S.s1[1] = anchor1;
+                    S.s1[2] = anchor2;
+                }
+                const double an[3] = {anchor0, anchor1, anchor2};
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int b = lane + 32 * q;
+                    if (b < N - 1)
+                        for (int d = 0; d < 3; ++d) S.s1[3 * (b + 1) + d] = an[d] + scan[q][d];
+                }
+                __syncwarp();
+                W.load(S.s1, Rc);
+                __syncwarp();
+                double s = 0.0;
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    if (W.valid(q)) {
+                        const double e0 = Rc[q][0] - Rprev[q][0], e1 = Rc[q][1] - Rprev[q][1],
+                                     e2 = Rc[q][2] - Rprev[q][2];
+                        s += e0 * e0 + e1 * e1 + e2 * e2;
+                    }
+                const double incr = sqrt(wsum(s)) / N;
+                W.cnt[C_CORR] += 1;
+                if (incr < ch.tol) break;
+                if (!(incr == incr) || isinf(incr)) {
+                    W.status |= BDCU_ST_NONFINITE;
+                    break;
+                }
+                if (iter >= max_iter) {
+                    W.status |= BDCU_ST_NONCONVERGED;
+                    W.cnt[C_NONCONV] += 1;
+                    break;
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) Rprev[q][d] = Rc[q][d];
+            }
+            // every lane's connector status, then a warp-uniform fatal test
+            W.status |= __reduce_or_sync(kFull, lstat);
+            if (W.status & BDCU_ST_FATAL_MASK) break;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) R[q][d] = Rc[q][d];
+            W.cnt[C_STEPS] += 1;
+            t += dt;
+        }
+        if (!(W.status & BDCU_ST_FATAL_MASK)) W.store(gR, R);
+        if (lane == 0) {
+            a.rng[3 * c] = (int32_t)ux;
+            a.rng[3 * c + 1] = iy;
+            a.rng[3 * c + 2] = seed;
+            a.cache_valid[c] = cache_valid;
+            a.status[c] = W.status;
+            int64_t* cc = reinterpret_cast<int64_t*>(a.counters + c);
+            for (int k = 0; k < 8; ++k) cc[k] += W.cnt[k];
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace bdcu

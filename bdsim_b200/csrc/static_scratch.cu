@@ -29,12 +29,15 @@
 
 #include "ctx.h"
 #include "integrator.cuh"
+#include "warp_layout.h"
 
 namespace bdcu {
 cudaError_t launch_plain(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t launch_mixed(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t occupancy_plain(int block, size_t smem, int* per_sm);
 cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm);
+cudaError_t launch_mixed_warp(const RunArgs& a, int grid, size_t smem, cudaStream_t s);
+cudaError_t occupancy_mixed_warp(size_t smem, int* per_sm);
 DevChain derive_record(const bdcu_phys& p, const bdcu_sim& s, int64_t bead_off);
 }  // namespace bdcu
 
@@ -67,6 +70,91 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 int fail(bdcu_ctx* c, int code, const std::string& msg) {
     c->err = msg;
     return code;
+}
+
+// The one-chain-per-warp mixed form, as bdcu_run dispatches it; the RNG
+// jump-ahead rows k = 0..n_max it reads are staged into the array too.
+int run_static_warp(bdcu_ctx* ctx, int n_chains, const std::vector<DevChain>& recs, const std::vector<double>& seed,
+                    const double* arena, int64_t arena_len, int n_max, int any_hi, int any_cheb, double* R,
+                    int32_t* rng, double* cache, int32_t* cache_valid, const double* t_start,
+                    const int32_t* n_steps, int32_t* status, bdcu_counters* counters, int cache_mode) {
+    const size_t smem = (size_t)warp_smem_bytes(n_max);
+    if (smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: warp kernel shared memory too large");
+    int per_sm = 0;
+    cudaError_t e = occupancy_mixed_warp(smem, &per_sm);
+    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+    if (per_sm < 1) per_sm = 1;
+    std::vector<uint32_t> cols((size_t)(n_max + 1) * 32);
+    std::vector<uint32_t> apow(n_max + 1);
+    for (int i = 0; i < 32; ++i) cols[i] = 1u << i;
+    apow[0] = 1;
+    for (int k = 1; k <= n_max; ++k) {
+        for (int i = 0; i < 32; ++i) {
+            uint32_t u = cols[(size_t)(k - 1) * 32 + i];
+            u ^= (u << 13);
+            u ^= (u >> 17);
+            u ^= (u << 5);
+            cols[(size_t)k * 32 + i] = u;
+        }
+        apow[k] = (uint32_t)(((uint64_t)apow[k - 1] * 16807ull) % 2147483647ull);
+    }
+    const size_t o_cnt = 0;
+    const size_t o_rec = 256;
+    const size_t o_seed = align256(o_rec + sizeof(DevChain) * (size_t)n_chains);
+    const size_t o_arena = align256(o_seed + sizeof(double) * (size_t)n_max);
+    const size_t o_cols = align256(o_arena + sizeof(double) * (size_t)std::max<int64_t>(arena_len, 1));
+    const size_t o_apow = align256(o_cols + sizeof(uint32_t) * cols.size());
+    const size_t o_scr = align256(o_apow + sizeof(uint32_t) * apow.size());
+    const int64_t wstride = any_hi ? warp_scratch_doubles(n_max) : 1;
+    const size_t per_block = sizeof(double) * (size_t)wstride * kWarpsPerCta;
+    if (o_scr + per_block > kStaticScratchBytes)
+        return fail(ctx, BDCU_E_LIMIT,
+                    "bdcu_run_static: needs " + std::to_string(o_scr + per_block) + " bytes of static device scratch "
+                    "for this batch (parameters plus one block's scratch); the maximum is " +
+                    std::to_string(kStaticScratchBytes) + " bytes. Use bdcu_run, or fewer/smaller chains.");
+    int grid = std::min((n_chains + kWarpsPerCta - 1) / kWarpsPerCta, per_sm * ctx->sm_count);
+    grid = (int)std::min<size_t>((size_t)grid, (kStaticScratchBytes - o_scr) / per_block);
+    if (grid < 1) grid = 1;
+    void* base = nullptr;
+    e = static_base(ctx->device, &base);
+    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    unsigned char* b = static_cast<unsigned char*>(base);
+    cudaStream_t s = ctx->stream;
+    e = cudaMemsetAsync(b + o_cnt, 0, sizeof(int32_t), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_rec, recs.data(), sizeof(DevChain) * n_chains, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_seed, seed.data(), sizeof(double) * n_max, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && arena_len > 0)
+        e = cudaMemcpyAsync(b + o_arena, arena, sizeof(double) * arena_len, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_cols, cols.data(), sizeof(uint32_t) * cols.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_apow, apow.data(), sizeof(uint32_t) * apow.size(), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("staging parameters: ") + cudaGetErrorString(e));
+    RunArgs a;
+    memset(&a, 0, sizeof(a));
+    a.chains = reinterpret_cast<const DevChain*>(b + o_rec);
+    a.n_chains = n_chains;
+    a.n_max = n_max;
+    a.arena = reinterpret_cast<const double*>(b + o_arena);
+    a.seed_table = reinterpret_cast<const double*>(b + o_seed);
+    a.R = R;
+    a.rng = rng;
+    a.cache = cache;
+    a.cache_valid = cache_valid;
+    a.t_start = t_start;
+    a.n_steps = n_steps;
+    a.status = status;
+    a.counters = counters;
+    a.cache_mode = cache_mode;
+    a.need_chol = any_hi;
+    a.need_d = any_hi;
+    a.need_lz = any_cheb;
+    a.work_counter = reinterpret_cast<int32_t*>(b + o_cnt);
+    a.scratch = reinterpret_cast<double*>(b + o_scr);
+    a.scratch_stride = wstride;
+    a.xs_pow = reinterpret_cast<const uint32_t*>(b + o_cols);
+    a.a_pow = reinterpret_cast<const uint32_t*>(b + o_apow);
+    e = launch_mixed_warp(a, grid, smem, s);
+    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("integrate kernel launch: ") + cudaGetErrorString(e));
+    return BDCU_OK;
 }
 
 }  // namespace
@@ -111,6 +199,13 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
     }
     std::vector<double> seed(n_max);
     for (int i = 0; i < n_max; ++i) seed[i] = sin(0.7654321 * (i + 1)) + 0.5;
+
+    int any_chol_method = 0;
+    for (int i = 0; i < n_chains; ++i)
+        if (phys[i].hstar > 0.0 && phys[i].hi_method == BDCU_HI_CHOLESKY) any_chol_method = 1;
+    if (form == BDCU_FORM_MIXED_FP32 && n_max <= kWarpMaxn && !any_chol_method)
+        return run_static_warp(ctx, n_chains, recs, seed, arena, arena_len, n_max, any_hi, any_cheb, R, rng, cache,
+                               cache_valid, t_start, n_steps, status, counters, cache_mode);
 
     // launch shape, as bdcu_run plans it
     const int mixed = (form == BDCU_FORM_MIXED_FP32);
