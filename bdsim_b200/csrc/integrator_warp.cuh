@@ -74,19 +74,20 @@ static __device__ void halfwarp_bisect(const double* al, const double* bb, int k
             if (d == 0) nb = m; else na = m;
             node = 2 * node + 1 + d;
         }
-        const bool same = (na == lo && nb == hi);
+        // settled: the interval stopped shrinking or is within 1e-10 relative
+        // (the bounds are padded by 2x / 2% downstream)
+        const bool done = (na == lo && nb == hi) || (nb - na) <= 1e-10 * fmax(fabs(na), fabs(nb));
         lo = na;
         hi = nb;
-        // both half warps keep iterating until both are settled
-        if (__all_sync(kFull, same)) break;
+        if (__all_sync(kFull, done)) break;
     }
 }
 
 // Inverse iteration for a Ritz vector (src/hydrodynamics.cpp:106-136), one lane.
-static __device__ void wk_tridiag_vec(const double* a, const double* b, int m, double lambda, double* y) {
+static __device__ void wk_tridiag_vec(const double* a, const double* b, int m, double lambda, double* y, double* c,
+                                      double* d) {
     const double scale = dmax_(fabs(lambda), 1.0);
     const double shift = lambda - 1.0e-7 * scale;
-    double c[kLanczosCold], d[kLanczosCold];
     const double y0 = rsqrt((double)m);
     for (int i = 0; i < m; ++i) y[i] = y0;
     for (int it = 0; it < 2; ++it) {
@@ -121,6 +122,8 @@ struct WarpChain {
     WarpShared& S;
     const DevChain& ch;
     double* V;      // warm Lanczos basis in shared memory (kLanczosWarm x nv)
+    float* sqx;     // Chebyshev node values, aliasing V (dead after the bounds)
+    float* coef;    // Chebyshev coefficients, aliasing V
     double* Vg;     // cold basis in global scratch (kLanczosCold x nv)
     double* Lt;     // Cholesky factor in global scratch (n x n)
     int nv;
@@ -129,8 +132,10 @@ struct WarpChain {
     bool hi;
     int64_t cnt[8];
     int status;
-    // RPY constants (FP32)
-    float hs, TRPIhs, K1, K2, K3, C3ihs, C7ihs;
+    // RPY constants (FP32). Bead coordinates are staged divided by `scale`
+    // (= h* under HI), which turns the RPY weights into functions of
+    // rho = h*/r alone.
+    float scale, iscale, K1, K2, K3, C3, C7;
 
     __device__ WarpChain(const RunArgs& a_, WarpShared& S_, const DevChain& ch_) : a(a_), S(S_), ch(ch_) {}
 
@@ -138,44 +143,38 @@ struct WarpChain {
 
     // ---- FP32 matrix-free D.x (Diffusion::apply, src/mobility.cpp:53-56;
     // RPY weights src/hydrodynamics.cpp:77-105). x, y: the lane's two beads.
-    __device__ void apply(const double (&x)[2][3], double (&y)[2][3]) {
-        if (!hi) {
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) y[q][d] = x[q][d];
-            return;
-        }
+    __device__ void apply32(const float (&x)[2][3], float (&acc)[2][3]) {
         cnt[C_DX] += 1;
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-            if (valid(q)) S.xs[lane + 32 * q] = make_float4((float)x[q][0], (float)x[q][1], (float)x[q][2], 0.f);
+            if (valid(q)) S.xs[lane + 32 * q] = make_float4(x[q][0], x[q][1], x[q][2], 0.f);
         __syncwarp();
-        float acc[2][3];
         float4 pb[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             pb[q] = valid(q) ? S.pos[lane + 32 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) acc[q][d] = (float)x[q][d];
+            for (int d = 0; d < 3; ++d) acc[q][d] = 0.f;
         }
+        // In units of h*: with d = (R_j - R_b)/h*, s = |d|^2, rho = s^-1/2,
+        //   far  (s >= 4 pi): om1 = rho (K1 + K2 rho^2), om2 = rho^3 (K1 - K3 rho^2)
+        //   near (s <  4 pi): om1 = 1 - C3 s rho,         om2 = C7 rho
+        // and y_b += om1 x_j + om2 (d.x_j) d. The self pair (d = 0, s clamped
+        // to 1e-24) takes the near branch with om1 = 1 exactly in FP32 and
+        // om2 d = 0: it contributes the identity block.
+#pragma unroll 2
         for (int j = 0; j < N; ++j) {
             const float4 pj = S.pos[j];
             const float4 xj = S.xs[j];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
-                const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
-                const float rinv = rsqrtf(sq);
-                const float rs = sq * rinv;
-                const float hr = hs * rinv;
-                const float hr2 = hr * hr;
-                const bool far = rs >= TRPIhs;
-                float om1 = far ? hr * (K1 + K2 * hr2) : 1.f - C3ihs * rs;
-                float om2 = far ? hr * rinv * rinv * (K1 - K3 * hr2) : C7ihs * rs * rinv * rinv;
-                const bool self = (j == lane + 32 * q);
-                om1 = self ? 0.f : om1;
-                om2 = self ? 0.f : om2;
+                const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
+                const float rho = rsqrtf(sq);
+                const float rho2 = rho * rho;
+                const bool far = sq >= 12.566370614359172f;
+                const float om1 = far ? rho * (K1 + K2 * rho2) : 1.f - C3 * (sq * rho);
+                const float om2 = far ? (rho * rho2) * (K1 - K3 * rho2) : C7 * rho;
                 const float t = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
                 acc[q][0] += om1 * xj.x + t * dx;
                 acc[q][1] += om1 * xj.y + t * dy;
@@ -185,8 +184,50 @@ struct WarpChain {
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
+            if (!valid(q))
 #pragma unroll
-            for (int d = 0; d < 3; ++d) y[q][d] = valid(q) ? (double)acc[q][d] : 0.0;
+                for (int d = 0; d < 3; ++d) acc[q][d] = 0.f;
+    }
+
+    __device__ void apply(const double (&x)[2][3], double (&y)[2][3]) {
+        if (!hi) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) y[q][d] = x[q][d];
+            return;
+        }
+        float xf[2][3], yf[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) xf[q][d] = (float)x[q][d];
+        apply32(xf, yf);
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) y[q][d] = (double)yf[q][d];
+    }
+
+    // D.x on FP32 lane vectors (identity without HI).
+    __device__ void applyF(const float (&x)[2][3], float (&y)[2][3]) {
+        if (!hi) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) y[q][d] = x[q][d];
+            return;
+        }
+        apply32(x, y);
+    }
+
+    __device__ double dotf(const float (&x)[2][3], const float (&y)[2][3]) const {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) s += (double)x[q][d] * (double)y[q][d];
+        return wsum(s);
     }
 
     __device__ double dot(const double (&x)[2][3], const double (&y)[2][3]) const {
@@ -202,7 +243,9 @@ struct WarpChain {
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-            if (valid(q)) S.pos[lane + 32 * q] = make_float4((float)R[q][0], (float)R[q][1], (float)R[q][2], 0.f);
+            if (valid(q))
+                S.pos[lane + 32 * q] = make_float4((float)(R[q][0] * iscale), (float)(R[q][1] * iscale),
+                                                   (float)(R[q][2] * iscale), 0.f);
         __syncwarp();
     }
 
@@ -218,7 +261,7 @@ struct WarpChain {
     // Fs: spring bead forces (src/spring.cpp:195-207). Fe: (EV + bending) +
     // external(t) (src/model.hpp:56-64). Positions must be staged (S.pos) and
     // R copied to S.s0.
-    __device__ void forces(const double (&R)[2][3], double t, double (&Fs)[2][3], double (&Fe)[2][3], bool spring) {
+    __device__ void forces(const double (&R)[2][3], double t, float (&Fs)[2][3], float (&Fe)[2][3], bool spring) {
         to_smem(S.s0, R);
         __syncwarp();
         // bonds b = lane, lane+32 (b < N-1): Fc -> s1, unit bonds -> s2, lengths -> s3
@@ -252,13 +295,59 @@ struct WarpChain {
             }
             __syncwarp();
         }
-        const float zs = (float)ch.zsbyds5, p5 = (float)ch.pt5bydssq;
+        // EV on the scaled coordinates: r = scale*|d|, force -fac(r) * scale * d
+        // EV on the scaled coordinates: r = scale*|d|, force -fac(r) * scale * d
+        const float zs = (float)(ch.zsbyds5 * scale), p5 = (float)(ch.pt5bydssq * (double)scale * scale);
         const double* phi = (ch.ev_type == BDCU_EV_SDK && ch.phi_off >= 0) ? a.arena + ch.phi_off : nullptr;
+        // excluded volume, FP32 pair sums over both bead slots at once: the
+        // force on m from j is -fac(r) (R_j - R_m), |j - m| >= contour distance
+        float fev[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        if (ch.ev_type == BDCU_EV_GAUSS) {
+            float4 pm[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) pm[q] = valid(q) ? S.pos[lane + 32 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const int cd = ch.cd;
+#pragma unroll 2
+            for (int j = 0; j < N; ++j) {
+                const float4 pj = S.pos[j];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int m = lane + 32 * q;
+                    const float dx = pj.x - pm[q].x, dy = pj.y - pm[q].y, dz = pj.z - pm[q].z;
+                    const float sq = dx * dx + dy * dy + dz * dz;
+                    const int dj = j > m ? j - m : m - j;
+                    const float fac = (dj >= cd && j != m) ? zs * __expf(-sq * p5) : 0.f;
+                    fev[q][0] -= fac * dx;
+                    fev[q][1] -= fac * dy;
+                    fev[q][2] -= fac * dz;
+                }
+            }
+        } else if (ch.ev_type != BDCU_EV_NONE) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int m = lane + 32 * q;
+                if (!valid(q)) continue;
+                const float4 pm = S.pos[m];
+                for (int j = 0; j < N; ++j) {
+                    const int dj = j > m ? j - m : m - j;
+                    if (dj < ch.cd || j == m) continue;
+                    const float4 pj = S.pos[j];
+                    const float dx = pj.x - pm.x, dy = pj.y - pm.y, dz = pj.z - pm.z;
+                    const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
+                    const int mu = j < m ? j : m, nu = j < m ? m : j;
+                    const float fac =
+                        (float)(ev_factor(ch, sqrt((double)sq) * scale, phi ? phi[mu * N + nu] : 0.0) * scale);
+                    fev[q][0] -= fac * dx;
+                    fev[q][1] -= fac * dy;
+                    fev[q][2] -= fac * dz;
+                }
+            }
+        }
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int m = lane + 32 * q;
             if (!valid(q)) {
-                for (int d = 0; d < 3; ++d) Fs[q][d] = Fe[q][d] = 0.0;
+                for (int d = 0; d < 3; ++d) Fs[q][d] = Fe[q][d] = 0.f;
                 continue;
             }
             if (spring) {
@@ -267,38 +356,15 @@ struct WarpChain {
                     if (m == 0) v = S.s1[d];
                     else if (m == N - 1) v = -S.s1[3 * (N - 2) + d];
                     else v = S.s1[3 * m + d] - S.s1[3 * (m - 1) + d];
-                    Fs[q][d] = v;
-                }
-            }
-            // excluded volume, FP32 pair sums: the force on m from j is
-            // -fac(r) (R_j - R_m), |j - m| >= contour distance
-            float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-            if (ch.ev_type != BDCU_EV_NONE) {
-                const float4 pm = S.pos[m];
-                for (int j = 0; j < N; ++j) {
-                    const int dj = j > m ? j - m : m - j;
-                    if (dj < ch.cd || j == m) continue;
-                    const float4 pj = S.pos[j];
-                    const float dx = pj.x - pm.x, dy = pj.y - pm.y, dz = pj.z - pm.z;
-                    const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
-                    float fac;
-                    if (ch.ev_type == BDCU_EV_GAUSS) {
-                        fac = zs * __expf(-sq * p5);
-                    } else {
-                        const int mu = j < m ? j : m, nu = j < m ? m : j;
-                        fac = (float)ev_factor(ch, sqrt((double)sq), phi ? phi[mu * N + nu] : 0.0);
-                    }
-                    f0 -= fac * dx;
-                    f1 -= fac * dy;
-                    f2 -= fac * dz;
+                    Fs[q][d] = (float)v;
                 }
             }
             double fb[3] = {0.0, 0.0, 0.0}, fx[3] = {0.0, 0.0, 0.0};
             if (bend) bending_on_bead(ch, m, S.s2, S.s4, S.s3, fb);
             if (ch.ext_n > 0) external_on_bead(ch, a.arena, m, t, fx);
-            Fe[q][0] = ((double)f0 + fb[0]) + fx[0];
-            Fe[q][1] = ((double)f1 + fb[1]) + fx[1];
-            Fe[q][2] = ((double)f2 + fb[2]) + fx[2];
+            Fe[q][0] = (float)(((double)fev[q][0] + fb[0]) + fx[0]);
+            Fe[q][1] = (float)(((double)fev[q][1] + fb[1]) + fx[1]);
+            Fe[q][2] = (float)(((double)fev[q][2] + fb[2]) + fx[2]);
         }
         __syncwarp();
     }
@@ -306,7 +372,7 @@ struct WarpChain {
     // ---- noise: the 3N draws of raw_noise (src/mobility.cpp:18-29) -------
     // 32 lanes draw contiguous blocks of the stream; lane l jumps to draw l*c
     // with the tabulated powers, so the uniforms equal ran_1's, bit for bit.
-    __device__ void noise(uint32_t& ux0, int32_t& iy0, int32_t& seed, double (&X)[2][3]) {
+    __device__ void noise(uint32_t& ux0, int32_t& iy0, int32_t& seed, float (&X)[2][3]) {
         if (seed <= 0 || iy0 < 0) {
             const int32_t s = seed < 0 ? -seed : seed;
             iy0 = (888889999 ^ s) | 1;
@@ -349,7 +415,7 @@ struct WarpChain {
                     const double y = S.s0[3 * (lane + 32 * q) + d] - 0.5;
                     v = (14.14855378 * y * y + 1.21569221) * y;
                 }
-                X[q][d] = v;
+                X[q][d] = (float)v;
             }
         __syncwarp();
     }
@@ -401,8 +467,63 @@ struct WarpChain {
             for (int d = 0; d < 3; ++d) vp[q][d] = 0.0;
         int k = 0;
         double b = 0.0;
+        if (m <= kLanczosWarm) {
+            // warm runs: classical Gram-Schmidt applied twice against the whole
+            // basis, each pass's projections reduced together; the projection
+            // on v_j is alpha_j
+            for (int j = 0; j < m; ++j) {
+                store(basis(j, m), v);
+                apply(v, w);
+                double al = 0.0;
+                for (int pass = 0; pass < 2; ++pass) {
+                    double c[kLanczosWarm];
+#pragma unroll
+                    for (int u = 0; u < kLanczosWarm; ++u) {
+                        c[u] = 0.0;
+                        if (u <= j) {
+                            const double* vu = basis(u, m);
+#pragma unroll
+                            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                                for (int d = 0; d < 3; ++d)
+                                    if (valid(q)) c[u] += w[q][d] * vu[3 * (lane + 32 * q) + d];
+                        }
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                        for (int u = 0; u < kLanczosWarm; ++u) c[u] += __shfl_xor_sync(kFull, c[u], o);
+#pragma unroll
+                    for (int u = 0; u < kLanczosWarm; ++u) {
+                        if (u <= j) {
+                            const double* vu = basis(u, m);
+#pragma unroll
+                            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                                for (int d = 0; d < 3; ++d)
+                                    if (valid(q)) w[q][d] -= c[u] * vu[3 * (lane + 32 * q) + d];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kLanczosWarm; ++u)
+                        if (u == j) al += c[u];
+                }
+                if (lane == 0) S.alpha[k] = al;
+                ++k;
+                b = sqrt(dot(w, w));
+                if (b < 1.0e-10) break;
+                const double ib = 1.0 / b;
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) v[q][d] = w[q][d] * ib;
+                if (lane == 0) S.beta[j] = b;
+            }
+        } else {
+        // cold runs (first step of a call): the reference's modified Gram-Schmidt
         for (int j = 0; j < m; ++j) {
             store(basis(j, m), v);
+
             apply(v, w);
             const double al = dot(v, w);
             if (lane == 0) S.alpha[k] = al;
@@ -433,6 +554,7 @@ struct WarpChain {
                 }
             if (lane == 0) S.beta[j] = b;
         }
+        }
         __syncwarp();
         if (k == 1) {
             rmin = rmax = S.alpha[0];
@@ -452,8 +574,11 @@ struct WarpChain {
         const double r = 0.5 * (l2 + h2);
         rmin = __shfl_sync(kFull, r, 0);
         rmax = __shfl_sync(kFull, r, 16);
-        if (lane == 0) wk_tridiag_vec(S.alpha, S.beta, k, rmin, S.ymin);
-        if (lane == 16) wk_tridiag_vec(S.alpha, S.beta, k, rmax, S.ymax);
+        if (lane == 0 || lane == 16) {
+            const bool lo_end = lane == 0;
+            wk_tridiag_vec(S.alpha, S.beta, k, lo_end ? rmin : rmax, lo_end ? S.ymin : S.ymax,
+                           lo_end ? S.s3 : S.s3 + 32, lo_end ? S.s4 : S.s4 + 32);
+        }
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
@@ -514,10 +639,10 @@ struct WarpChain {
 
     // ---- Chebyshev square root, FP32 recurrence (src/hydrodynamics.cpp:267-337)
     // Returns the FD error; out = approx D^{1/2} x0.
-    __device__ double chebyshev(const double (&x0)[2][3], double lmin, double lmax, double (&out)[2][3]) {
-        double Dx0[2][3];
-        apply(x0, Dx0);
-        const double x0Dx0 = dot(x0, Dx0);
+    __device__ double chebyshev(const float (&x0)[2][3], double lmin, double lmax, float (&out)[2][3]) {
+        float Dx0[2][3];
+        apply32(x0, Dx0);
+        const double x0Dx0 = dotf(x0, Dx0);
         double Lr = sqrt(lmax / lmin) * ch.mult + 0.5;
         int L = !(Lr < 2.0e9) ? kMaxCheb : (int)Lr + 1;
         L = L > kMaxCheb ? kMaxCheb : (L < 2 ? 2 : L);
@@ -526,42 +651,39 @@ struct WarpChain {
         double fd = 0.0;
         for (;;) {
             const float inv = 1.f / (float)(L + 1);
+            const float ida = 1.f / da;
             for (int k = lane; k <= L; k += 32) {
-                const float xk = cospif(((float)k + 0.5f) * inv) / da - db / da;
-                S.sqx[k] = sqrtf(xk);
+                const float xk = (cospif(((float)k + 0.5f) * inv) - db) * ida;
+                sqx[k] = sqrtf(xk);
             }
             __syncwarp();
             for (int j = lane; j <= L; j += 32) {
                 float s = 0.f;
-                for (int k = 0; k <= L; ++k) s += S.sqx[k] * cospif((float)j * ((float)k + 0.5f) * inv);
+                for (int k = 0; k <= L; ++k) s += sqx[k] * cospif((float)j * ((float)k + 0.5f) * inv);
                 s *= 2.f * inv;
                 if (j == 0) s *= 0.5f;
-                S.coef[j] = s;
+                coef[j] = s;
             }
             __syncwarp();
             float tp[2][3], tc[2][3], o[2][3];
-            const float c0 = S.coef[0], c1 = S.coef[1];
+            const float c0 = coef[0], c1 = coef[1];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    tp[q][d] = (float)x0[q][d];
-                    tc[q][d] = da * (float)Dx0[q][d] + db * tp[q][d];
+                    tp[q][d] = x0[q][d];
+                    tc[q][d] = da * Dx0[q][d] + db * tp[q][d];
                     o[q][d] = c0 * tp[q][d] + c1 * tc[q][d];
                 }
             for (int l = 2; l <= L; ++l) {
-                double tcd[2][3], Dv[2][3];
-#pragma unroll
-                for (int q = 0; q < 2; ++q)
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) tcd[q][d] = tc[q][d];
-                apply(tcd, Dv);
-                const float cl = S.coef[l];
+                float Dv[2][3];
+                apply32(tc, Dv);
+                const float cl = coef[l];
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
-                        const float tn = 2.f * (da * (float)Dv[q][d] + db * tc[q][d]) - tp[q][d];
+                        const float tn = 2.f * (da * Dv[q][d] + db * tc[q][d]) - tp[q][d];
                         tp[q][d] = tc[q][d];
                         tc[q][d] = tn;
                         o[q][d] += cl * tn;
@@ -571,8 +693,8 @@ struct WarpChain {
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) out[q][d] = valid(q) ? (double)o[q][d] : 0.0;
-            const double rr = dot(out, out);
+                for (int d = 0; d < 3; ++d) out[q][d] = valid(q) ? o[q][d] : 0.f;
+            const double rr = dotf(out, out);
             fd = fabs(rr - x0Dx0) / x0Dx0;
             __syncwarp();
             if (fd <= ch.fd_tol || L >= kMaxCheb) break;
@@ -584,7 +706,7 @@ struct WarpChain {
 
     // ---- Cholesky fallback (src/mobility.cpp:69-81): dense FP64 D in global
     // scratch, right-looking factor, L x0. Returns false if not PD.
-    __device__ bool cholesky_noise(const double (&R)[2][3], const double (&x0)[2][3], double (&out)[2][3]) {
+    __device__ bool cholesky_noise(const double (&R)[2][3], const float (&x0)[2][3], float (&out)[2][3]) {
         to_smem(S.s0, R);
         __syncwarp();
         double* L = Lt;
@@ -626,7 +748,11 @@ struct WarpChain {
             }
             __syncwarp();
         }
-        to_smem(S.s1, x0);
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (valid(q))
+#pragma unroll
+                for (int d = 0; d < 3; ++d) S.s1[3 * (lane + 32 * q) + d] = (double)x0[q][d];
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
@@ -636,7 +762,7 @@ struct WarpChain {
                 double s = 0.0;
                 if (valid(q))
                     for (int j = 0; j <= i; ++j) s += L[(int64_t)j * n + i] * S.s1[j];
-                out[q][d] = s;
+                out[q][d] = (float)s;
             }
         __syncwarp();
         return true;
@@ -645,7 +771,7 @@ struct WarpChain {
 
 // -------------------------------------------------------------- the kernel
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const RunArgs a) {
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(const RunArgs a) {
     extern __shared__ __align__(16) unsigned char wsm[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -677,6 +803,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
         }
         WarpChain W(a, S, ch);
         W.V = Vs;
+        W.sqx = reinterpret_cast<float*>(Vs);
+        W.coef = reinterpret_cast<float*>(Vs) + kCoefCap;
         W.Vg = scr;
         W.Lt = scr + (int64_t)kLanczosCold * nvr;
         W.nv = nvr;
@@ -687,15 +815,15 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
         W.status = status;
         for (int k = 0; k < 8; ++k) W.cnt[k] = 0;
         {
-            const float RPI = 1.7724538509055160f, TPI = 6.283185307179586f;
-            const float hsf = (float)ch.hstar;
-            W.hs = hsf;
-            W.TRPIhs = 2.f * RPI * hsf;
-            W.K1 = RPI * 0.75f;
-            W.K2 = RPI * 0.75f * (TPI / 3.f);
-            W.K3 = RPI * 0.75f * TPI;
-            W.C3ihs = (0.75f / RPI * 0.375f) / hsf;
-            W.C7ihs = (0.09375f / RPI) / hsf;
+            const double RPI = 1.7724538509055160, TPI = 6.283185307179586;
+            const double K1 = RPI * 0.75;
+            W.scale = ch.hstar > 0.0 ? (float)ch.hstar : 1.f;
+            W.iscale = 1.f / W.scale;
+            W.K1 = (float)K1;
+            W.K2 = (float)(K1 * (TPI / 3.0));
+            W.K3 = (float)(K1 * TPI);
+            W.C3 = (float)(0.75 / RPI * 0.375);
+            W.C7 = (float)(0.09375 / RPI);
         }
         const int N = W.N;
         double* gR = a.R + 3 * ch.bead_off;
@@ -726,18 +854,19 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
                         for (int d = 0; d < 3; ++d) R[q][d] -= com[d];
             }
             W.stage_pos(R);
-            double Fs[2][3], Fe[2][3];
+            float Fs[2][3], Fe[2][3];
             W.forces(R, t, Fs, Fe, true);
-            double X0[2][3], dW[2][3];
+            float X0[2][3], dW[2][3];
             W.noise(ux, iy, seed, X0);
             // brownian_step (src/mobility.cpp:58-88)
             if (!W.hi) {
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) dW[q][d] = sqrt_dt * X0[q][d];
+                    for (int d = 0; d < 3; ++d) dW[q][d] = (float)(sqrt_dt * X0[q][d]);
             } else {
-                double lmin, lmax, bx[2][3];
+                double lmin, lmax;
+                float bx[2][3];
                 W.bounds(gcache, cache_valid, lmin, lmax);
                 const double fd = W.chebyshev(X0, lmin, lmax, bx);
                 if (!(fd <= ch.fd_tol)) {
@@ -751,18 +880,19 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) dW[q][d] = sqrt_dt * bx[q][d];
+                    for (int d = 0; d < 3; ++d) dW[q][d] = (float)(sqrt_dt * bx[q][d]);
             }
             // predictor (src/integrator.cpp:96-101)
             double K1[9], K2[9];
             kappa_at(ch, a.arena, t, K1);
             kappa_at(ch, a.arena, t + dt, K2);
-            double A[2][3], DF[2][3], Rp[2][3];
+            float A[2][3], DF[2][3];
+            double Rp[2][3];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) A[q][d] = Fs[q][d] + Fe[q][d];
-            W.apply(A, DF);
+            W.applyF(A, DF);
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
@@ -772,16 +902,17 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
                 }
             // upsilon (src/integrator.cpp:107-119): forces at R~ with R~'s coordinates staged
             W.stage_pos(Rp);
-            double Fep[2][3], dummy[2][3];
+            float Fep[2][3], dummy[2][3];
             W.forces(Rp, t + dt, dummy, Fep, false);
             W.stage_pos(R);
-            double DFs[2][3], DFe[2][3], ups[2][3];
-            W.apply(Fs, DFs);
+            float DFs[2][3], DFe[2][3];
+            double ups[2][3];
+            W.applyF(Fs, DFs);
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) A[q][d] = Fe[q][d] + Fep[q][d];
-            W.apply(A, DFe);
+            W.applyF(A, DFe);
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
@@ -831,7 +962,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
                     }
                 }
                 __syncwarp();
-                double Fb[2][3], DFb[2][3];
+                float Fb[2][3], DFb[2][3];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const int m = lane + 32 * q;
@@ -843,12 +974,16 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) integrate_warp_kernel(const
                             else if (m == N - 1) v = -S.s1[3 * (N - 2) + d];
                             else v = S.s1[3 * m + d] - S.s1[3 * (m - 1) + d];
                         }
-                        Fb[q][d] = v;
+                        Fb[q][d] = (float)v;
                     }
                 }
                 __syncwarp();
-                W.apply(Fb, DFb);
-                W.to_smem(S.s2, DFb);
+                W.applyF(Fb, DFb);
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                    if (W.valid(q))
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) S.s2[3 * (lane + 32 * q) + d] = (double)DFb[q][d];
                 __syncwarp();
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
