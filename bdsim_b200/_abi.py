@@ -89,6 +89,16 @@ class BdcuCounters(ctypes.Structure):
 COUNTER_FIELDS = [f[0] for f in BdcuCounters._fields_]
 
 
+class BdcuBucketInfo(ctypes.Structure):
+    """One bucket of a launch plan (bdcu_bucket_info)."""
+    _fields_ = [(k, ctypes.c_int32) for k in (
+        "bucket", "kernel", "team_warps", "n_chains", "min_beads", "max_beads", "block", "grid", "v_cap",
+        "d_in_smem", "tuned", "reserved")] + [("smem_bytes", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class _Arena:
     def __init__(self):
         self.chunks = []
@@ -242,9 +252,18 @@ def load_library():
     lib.bdcu_ran1.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp]
     lib.bdcu_run_static.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim), c_double_p,
                                     ctypes.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
+    lib.bdcu_describe_plan.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BdcuBucketInfo), ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int)]
+    lib.bdcu_autotune.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
+    lib.bdcu_reserve.argtypes = [vp, ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
+    lib.bdcu_update_chains.argtypes = [vp, ctypes.c_int, c_int32_p, ctypes.POINTER(BdcuPhys),
+                                       ctypes.POINTER(BdcuSim), c_int64_p]
+    lib.bdcu_write_arena.argtypes = [vp, ctypes.c_int64, c_double_p, ctypes.c_int64]
+    lib.bdcu_select.argtypes = [vp, ctypes.c_int, c_int32_p]
     for name in ("bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
                  "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
-                 "bdcu_forces", "bdcu_ran1", "bdcu_run_static"):
+                 "bdcu_forces", "bdcu_ran1", "bdcu_run_static", "bdcu_describe_plan", "bdcu_autotune",
+                 "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select"):
         getattr(lib, name).restype = ctypes.c_int
     _LIB = lib
     return lib
@@ -254,7 +273,11 @@ def load_library():
 EXPORTED_SYMBOLS = [
     "bdcu_version", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_last_error",
     "bdcu_set_chains", "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host",
-    "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_run_static",
+    "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_describe_plan", "bdcu_autotune",
+    "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select", "bdcu_run_static",
 ]
+
+KERNEL_BLOCK, KERNEL_TEAM = 0, 1
+MAX_BUCKETS = 8
 
 F_SPRING, F_EV, F_BEND, F_EXTERNAL = 1, 2, 4, 8

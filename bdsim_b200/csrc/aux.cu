@@ -22,6 +22,10 @@ __global__ void __launch_bounds__(256) forces_kernel(const RunArgs a, const doub
             for (int i = threadIdx.x; i < nw; i += blockDim.x) dst[i] = src[i];
         }
         __syncthreads();
+        if (chs.N < 2) {  // an empty slot of a pool
+            __syncthreads();
+            continue;
+        }
         Block<BDCU_FORM_PLAIN_FP64> B(a, ctl, chs);
         const int N = chs.N, n = 3 * N;
         B.N = N;
@@ -117,6 +121,24 @@ __global__ void ran1_kernel(int n_chains, int32_t* rng, int n_per, double* out) 
 
 cudaError_t launch_ran1(int n_chains, int32_t* rng, int n_per, double* out, cudaStream_t s) {
     ran1_kernel<<<(n_chains + 127) / 128, 128, 0, s>>>(n_chains, rng, n_per, out);
+    return cudaGetLastError();
+}
+
+// Copy chain records into their pool slots: one block per record.
+__global__ void scatter_records_kernel(DevChain* __restrict__ dst, const DevChain* __restrict__ src,
+                                       const int32_t* __restrict__ slots, int count) {
+    const int i = blockIdx.x;
+    if (i >= count) return;
+    const int nw = (int)(sizeof(DevChain) / 8);
+    const double* s = reinterpret_cast<const double*>(src + i);
+    double* d = reinterpret_cast<double*>(dst + slots[i]);
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) d[w] = s[w];
+}
+
+cudaError_t launch_scatter_records(DevChain* dst, const DevChain* src, const int32_t* slots, int count,
+                                   cudaStream_t s) {
+    if (count < 1) return cudaSuccess;
+    scatter_records_kernel<<<count, 32, 0, s>>>(dst, src, slots, count);
     return cudaGetLastError();
 }
 

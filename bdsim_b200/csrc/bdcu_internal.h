@@ -70,11 +70,15 @@ struct RunArgs {
     int32_t need_d;         // some chain has HI (dense D in the plain form)
     int32_t need_lz;        // some chain uses the Chebyshev method (Lanczos)
     int32_t* work_counter;  // persistent-grid chain queue (zeroed before launch)
-    double* scratch;        // per-CTA (per-warp for the warp kernel) global scratch
-    int64_t scratch_stride; // doubles per CTA (per warp)
+    const int32_t* order;   // the launch's work list: chain indices, largest first (null: 0..n_work-1)
+    int32_t n_work;         // entries of the work list
+    double* scratch;        // per-CTA (per-team for the team kernel) global scratch
+    int64_t scratch_stride; // doubles per CTA (per team)
     const uint32_t* xs_pow; // xorshift step matrix powers: columns of M^k, 32 words per k
     const uint32_t* a_pow;  // 16807^k mod (2^31 - 1)
 };
+
+static_assert(sizeof(DevChain) % 8 == 0, "records are copied as doubles");
 
 constexpr int kMaxDraws = 3 * kMaxBeads;  // jump-ahead tables cover k = 0..kMaxDraws
 

@@ -89,20 +89,23 @@ __device__ __forceinline__ double warp_allsum(double v) {
     return v;
 }
 
-// Dot product over the block, same value returned to every thread. Order: a
-// fixed tree (not the reference's sequential order; differences are at the
-// last bit of each sum).
+// Dot product over the block, same value returned to every thread, in one
+// fixed order whatever the block size (so a chain's result does not depend on
+// the launch shape its bucket was given): 64 partial sums, partial v adding
+// a[i]*b[i] for i = v, v+64, ... in order, then a butterfly within each half
+// and the two halves added. Not the reference's sequential order; the
+// difference is at the last bit of each sum. Needs blockDim.x >= 64.
 static __device__ double block_dot(const double* a, const double* b, int n, double* red) {
     double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += a[i] * b[i];
-    s = warp_allsum(s);
+    if (threadIdx.x < 64)
+        for (int i = threadIdx.x; i < n; i += 64) s += a[i] * b[i];
     __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    if (threadIdx.x < 64) {
+        s = warp_allsum(s);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    }
     __syncthreads();
-    double t = 0.0;
-    const int nw = blockDim.x >> 5;
-    for (int w = 0; w < nw; ++w) t += red[w];
-    return t;
+    return red[0] + red[1];
 }
 
 // y = D x, one row per thread, summed over j in order (matvec,
@@ -731,10 +734,13 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
 
     const int tid = threadIdx.x;
     for (;;) {
-        if (tid == 0) ctl.chain = atomicAdd(a.work_counter, 1);
+        if (tid == 0) {
+            const int item = atomicAdd(a.work_counter, 1);
+            ctl.chain = item >= a.n_work ? -1 : (a.order ? a.order[item] : item);
+        }
         __syncthreads();
         const int c = ctl.chain;
-        if (c >= a.n_chains) break;
+        if (c < 0) break;
         {
             const int nw = (int)(sizeof(DevChain) / 8);
             const double* src = reinterpret_cast<const double*>(a.chains + c);

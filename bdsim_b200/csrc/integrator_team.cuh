@@ -1,23 +1,26 @@
-// integrator_warp.cuh -- the FP32-mixed form with one chain per WARP, for
-// chains of up to 64 beads. Each warp claims chains from the device work
-// queue and owns one chain at a time; lane l owns beads l and l+32, holding
-// their positions, forces and noise in registers. There is no block-wide
-// barrier: neighbour data (bonds, prefix sums) goes through the warp's own
-// shared-memory area under __syncwarp, reductions are warp shuffles.
+// integrator_team.cuh -- the FP32-mixed form with one chain per TEAM of T
+// warps (T = 1, 2, 4, 8), for chains of up to 64*T beads. Each team claims
+// chains from the device work queue and owns one chain at a time; team thread
+// u owns beads u and u + 32T, holding their positions, forces and noise in
+// registers. There is no block-wide barrier: neighbour data (bonds, prefix
+// sums) goes through the team's own shared-memory area under the team barrier
+// (__syncwarp for T = 1, a named barrier otherwise); reductions are warp
+// shuffles followed, for T > 1, by a fixed-order sum over the team's warps.
 //
 // Precision (the mixed form): D.x recomputed pairwise in FP32 from shared FP32
 // bead coordinates, FP32 excluded volume and Chebyshev recurrence; FP64
 // positions, spring/bending forces, connector solve, Lanczos vectors and
 // tridiagonal bounds, and the (rare) Cholesky fallback. The noise stream is
-// the reference's ran_1 stream bit for bit, drawn by 32 lanes at once with a
-// jump-ahead (GF(2) powers of the xorshift step, powers of 16807 mod 2^31-1).
+// the reference's ran_1 stream bit for bit, drawn by all team threads at once
+// with a jump-ahead (GF(2) powers of the xorshift step, powers of 16807 mod
+// 2^31-1).
 //
 // Reference: src/integrator.cpp:61-170 of the bdsim project and the physics it
 // calls; each stage cites its reference function.
 #pragma once
 
 #include "integrator.cuh"
-#include "warp_layout.h"
+#include "team_layout.h"
 
 namespace bdcu {
 
@@ -25,6 +28,17 @@ __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
     return v;
+}
+
+// Barrier over one team: __syncwarp for a single warp, else named barrier
+// 1 + team (barrier 0 is __syncthreads') over the team's 32T threads.
+template <int T>
+__device__ __forceinline__ void team_sync(int team) {
+    if constexpr (T == 1) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(32 * T) : "memory");
+    }
 }
 
 // Number of eigenvalues of the tridiagonal (a, b) below x, from the signs of
@@ -117,9 +131,12 @@ static __device__ void wk_tridiag_vec(const double* a, const double* b, int m, d
     }
 }
 
-struct WarpChain {
+
+template <int T>
+struct TeamChain {
+    static constexpr int TT = 32 * T;  // threads of the team
     const RunArgs& a;
-    WarpShared& S;
+    TeamShared<T>& S;
     const DevChain& ch;
     double* V;      // warm Lanczos basis in shared memory (kLanczosWarm x nv)
     float* sqx;     // Chebyshev node values, aliasing V (dead after the bounds)
@@ -127,7 +144,9 @@ struct WarpChain {
     double* Vg;     // cold basis in global scratch (kLanczosCold x nv)
     double* Lt;     // Cholesky factor in global scratch (n x n)
     int nv;
-    int lane;
+    int tid;        // thread in the team
+    int wl, wi;     // lane in its warp, warp in the team
+    int team;       // team in the thread block (named barrier 1 + team)
     int N, n;
     bool hi;
     int64_t cnt[8];
@@ -137,22 +156,79 @@ struct WarpChain {
     // rho = h*/r alone.
     float scale, iscale, K1, K2, K3, C3, C7;
 
-    __device__ WarpChain(const RunArgs& a_, WarpShared& S_, const DevChain& ch_) : a(a_), S(S_), ch(ch_) {}
+    __device__ TeamChain(const RunArgs& a_, TeamShared<T>& S_, const DevChain& ch_) : a(a_), S(S_), ch(ch_) {}
 
-    __device__ __forceinline__ bool valid(int q) const { return lane + 32 * q < N; }
+    __device__ __forceinline__ bool valid(int q) const { return tid + TT * q < N; }
+    __device__ __forceinline__ int bead(int q) const { return tid + TT * q; }
+    __device__ __forceinline__ void sync() const { team_sync<T>(team); }
+
+    // Sum over the team, the same bits in every thread: warp butterflies, then
+    // the warps' partial sums added in warp order.
+    __device__ double tsum(double v) const {
+        v = wsum(v);
+        if constexpr (T == 1) {
+            return v;
+        } else {
+            sync();
+            if (wl == 0) S.red[wi] = v;
+            sync();
+            double s = S.red[0];
+#pragma unroll
+            for (int w = 1; w < T; ++w) s += S.red[w];
+            return s;
+        }
+    }
+
+    // Eight team sums at once (the batched projections of the warm Lanczos).
+    __device__ void tsum8(double (&c)[kLanczosWarm]) const {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int u = 0; u < kLanczosWarm; ++u) c[u] += __shfl_xor_sync(kFull, c[u], o);
+        if constexpr (T > 1) {
+            sync();
+            if (wl == 0)
+#pragma unroll
+                for (int u = 0; u < kLanczosWarm; ++u) S.red[kLanczosWarm * wi + u] = c[u];
+            sync();
+#pragma unroll
+            for (int u = 0; u < kLanczosWarm; ++u) {
+                double s = S.red[u];
+#pragma unroll
+                for (int w = 1; w < T; ++w) s += S.red[kLanczosWarm * w + u];
+                c[u] = s;
+            }
+        }
+    }
+
+    // OR of status bits over the team.
+    __device__ int tor(int v) const {
+        v = __reduce_or_sync(kFull, v);
+        if constexpr (T == 1) {
+            return v;
+        } else {
+            sync();
+            if (wl == 0) S.flag[wi] = v;
+            sync();
+            int s = 0;
+#pragma unroll
+            for (int w = 0; w < T; ++w) s |= S.flag[w];
+            return s;
+        }
+    }
 
     // ---- FP32 matrix-free D.x (Diffusion::apply, src/mobility.cpp:53-56;
-    // RPY weights src/hydrodynamics.cpp:77-105). x, y: the lane's two beads.
+    // RPY weights src/hydrodynamics.cpp:77-105). x, y: the thread's two beads.
     __device__ void apply32(const float (&x)[2][3], float (&acc)[2][3]) {
         cnt[C_DX] += 1;
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-            if (valid(q)) S.xs[lane + 32 * q] = make_float4(x[q][0], x[q][1], x[q][2], 0.f);
-        __syncwarp();
+            if (valid(q)) S.xs[bead(q)] = make_float4(x[q][0], x[q][1], x[q][2], 0.f);
+        sync();
         float4 pb[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            pb[q] = valid(q) ? S.pos[lane + 32 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            pb[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int d = 0; d < 3; ++d) acc[q][d] = 0.f;
         }
@@ -162,26 +238,49 @@ struct WarpChain {
         // and y_b += om1 x_j + om2 (d.x_j) d. The self pair (d = 0, s clamped
         // to 1e-24) takes the near branch with om1 = 1 exactly in FP32 and
         // om2 d = 0: it contributes the identity block.
+        bool one_slot = false;
+        if constexpr (T > 1) one_slot = __all_sync(kFull, !valid(1));
+        if (one_slot) {
+            // the second bead slot is empty in every lane of this warp: only
+            // slot 0 does work (half the pairs)
 #pragma unroll 2
-        for (int j = 0; j < N; ++j) {
-            const float4 pj = S.pos[j];
-            const float4 xj = S.xs[j];
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
+            for (int j = 0; j < N; ++j) {
+                const float4 pj = S.pos[j];
+                const float4 xj = S.xs[j];
+                const float dx = pj.x - pb[0].x, dy = pj.y - pb[0].y, dz = pj.z - pb[0].z;
                 const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
                 const float rho = rsqrtf(sq);
                 const float rho2 = rho * rho;
                 const bool far = sq >= 12.566370614359172f;
                 const float om1 = far ? rho * (K1 + K2 * rho2) : 1.f - C3 * (sq * rho);
                 const float om2 = far ? (rho * rho2) * (K1 - K3 * rho2) : C7 * rho;
-                const float t = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
-                acc[q][0] += om1 * xj.x + t * dx;
-                acc[q][1] += om1 * xj.y + t * dy;
-                acc[q][2] += om1 * xj.z + t * dz;
+                const float tt = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
+                acc[0][0] += om1 * xj.x + tt * dx;
+                acc[0][1] += om1 * xj.y + tt * dy;
+                acc[0][2] += om1 * xj.z + tt * dz;
+            }
+        } else {
+#pragma unroll 2
+            for (int j = 0; j < N; ++j) {
+                const float4 pj = S.pos[j];
+                const float4 xj = S.xs[j];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
+                    const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
+                    const float rho = rsqrtf(sq);
+                    const float rho2 = rho * rho;
+                    const bool far = sq >= 12.566370614359172f;
+                    const float om1 = far ? rho * (K1 + K2 * rho2) : 1.f - C3 * (sq * rho);
+                    const float om2 = far ? (rho * rho2) * (K1 - K3 * rho2) : C7 * rho;
+                    const float tt = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
+                    acc[q][0] += om1 * xj.x + tt * dx;
+                    acc[q][1] += om1 * xj.y + tt * dy;
+                    acc[q][2] += om1 * xj.z + tt * dz;
+                }
             }
         }
-        __syncwarp();
+        sync();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
             if (!valid(q))
@@ -209,7 +308,7 @@ struct WarpChain {
             for (int d = 0; d < 3; ++d) y[q][d] = (double)yf[q][d];
     }
 
-    // D.x on FP32 lane vectors (identity without HI).
+    // D.x on FP32 thread vectors (identity without HI).
     __device__ void applyF(const float (&x)[2][3], float (&y)[2][3]) {
         if (!hi) {
 #pragma unroll
@@ -227,7 +326,7 @@ struct WarpChain {
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) s += (double)x[q][d] * (double)y[q][d];
-        return wsum(s);
+        return tsum(s);
     }
 
     __device__ double dot(const double (&x)[2][3], const double (&y)[2][3]) const {
@@ -236,38 +335,37 @@ struct WarpChain {
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) s += x[q][d] * y[q][d];
-        return wsum(s);
+        return tsum(s);
     }
 
     __device__ void stage_pos(const double (&R)[2][3]) {
-        __syncwarp();
+        sync();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
             if (valid(q))
-                S.pos[lane + 32 * q] = make_float4((float)(R[q][0] * iscale), (float)(R[q][1] * iscale),
-                                                   (float)(R[q][2] * iscale), 0.f);
-        __syncwarp();
+                S.pos[bead(q)] = make_float4((float)(R[q][0] * iscale), (float)(R[q][1] * iscale),
+                                             (float)(R[q][2] * iscale), 0.f);
+        sync();
     }
 
-    __device__ void to_smem(double* buf, const double (&x)[2][3]) {
+    __device__ void to_smem(double* buf, const double (&x)[2][3]) const {
 #pragma unroll
         for (int q = 0; q < 2; ++q)
             if (valid(q))
 #pragma unroll
-                for (int d = 0; d < 3; ++d) buf[3 * (lane + 32 * q) + d] = x[q][d];
+                for (int d = 0; d < 3; ++d) buf[3 * bead(q) + d] = x[q][d];
     }
 
     // ---- forces at R (FP64 springs/bending/external, FP32 EV) ------------
     // Fs: spring bead forces (src/spring.cpp:195-207). Fe: (EV + bending) +
-    // external(t) (src/model.hpp:56-64). Positions must be staged (S.pos) and
-    // R copied to S.s0.
+    // external(t) (src/model.hpp:56-64). Positions must be staged (S.pos).
     __device__ void forces(const double (&R)[2][3], double t, float (&Fs)[2][3], float (&Fe)[2][3], bool spring) {
         to_smem(S.s0, R);
-        __syncwarp();
-        // bonds b = lane, lane+32 (b < N-1): Fc -> s1, unit bonds -> s2, lengths -> s3
+        sync();
+        // bonds b = bead(0), bead(1) (b < N-1): Fc -> s1, unit bonds -> s2, lengths -> s3
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const int b = lane + 32 * q;
+            const int b = bead(q);
             if (b < N - 1) {
                 const double b0 = S.s0[3 * b + 3] - S.s0[3 * b], b1 = S.s0[3 * b + 4] - S.s0[3 * b + 1],
                              b2 = S.s0[3 * b + 5] - S.s0[3 * b + 2];
@@ -283,19 +381,18 @@ struct WarpChain {
                 S.s3[b] = len;
             }
         }
-        __syncwarp();
+        sync();
         const bool bend = ch.bend_type != BDCU_BEND_NONE && N > 2;
         if (bend) {
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                const int b = lane + 32 * q;
+                const int b = bead(q);
                 if (b < N - 2)
                     S.s4[b] = S.s2[3 * (b + 1)] * S.s2[3 * b] + S.s2[3 * (b + 1) + 1] * S.s2[3 * b + 1] +
                               S.s2[3 * (b + 1) + 2] * S.s2[3 * b + 2];
             }
-            __syncwarp();
+            sync();
         }
-        // EV on the scaled coordinates: r = scale*|d|, force -fac(r) * scale * d
         // EV on the scaled coordinates: r = scale*|d|, force -fac(r) * scale * d
         const float zs = (float)(ch.zsbyds5 * scale), p5 = (float)(ch.pt5bydssq * (double)scale * scale);
         const double* phi = (ch.ev_type == BDCU_EV_SDK && ch.phi_off >= 0) ? a.arena + ch.phi_off : nullptr;
@@ -305,14 +402,14 @@ struct WarpChain {
         if (ch.ev_type == BDCU_EV_GAUSS) {
             float4 pm[2];
 #pragma unroll
-            for (int q = 0; q < 2; ++q) pm[q] = valid(q) ? S.pos[lane + 32 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int q = 0; q < 2; ++q) pm[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
             const int cd = ch.cd;
 #pragma unroll 2
             for (int j = 0; j < N; ++j) {
                 const float4 pj = S.pos[j];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    const int m = lane + 32 * q;
+                    const int m = bead(q);
                     const float dx = pj.x - pm[q].x, dy = pj.y - pm[q].y, dz = pj.z - pm[q].z;
                     const float sq = dx * dx + dy * dy + dz * dz;
                     const int dj = j > m ? j - m : m - j;
@@ -325,7 +422,7 @@ struct WarpChain {
         } else if (ch.ev_type != BDCU_EV_NONE) {
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                const int m = lane + 32 * q;
+                const int m = bead(q);
                 if (!valid(q)) continue;
                 const float4 pm = S.pos[m];
                 for (int j = 0; j < N; ++j) {
@@ -345,7 +442,7 @@ struct WarpChain {
         }
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const int m = lane + 32 * q;
+            const int m = bead(q);
             if (!valid(q)) {
                 for (int d = 0; d < 3; ++d) Fs[q][d] = Fe[q][d] = 0.f;
                 continue;
@@ -366,12 +463,13 @@ struct WarpChain {
             Fe[q][1] = (float)(((double)fev[q][1] + fb[1]) + fx[1]);
             Fe[q][2] = (float)(((double)fev[q][2] + fb[2]) + fx[2]);
         }
-        __syncwarp();
+        sync();
     }
 
     // ---- noise: the 3N draws of raw_noise (src/mobility.cpp:18-29) -------
-    // 32 lanes draw contiguous blocks of the stream; lane l jumps to draw l*c
-    // with the tabulated powers, so the uniforms equal ran_1's, bit for bit.
+    // The team's threads draw contiguous blocks of the stream; thread u jumps
+    // to draw u*c with the tabulated powers, so the uniforms equal ran_1's,
+    // bit for bit.
     __device__ void noise(uint32_t& ux0, int32_t& iy0, int32_t& seed, float (&X)[2][3]) {
         if (seed <= 0 || iy0 < 0) {
             const int32_t s = seed < 0 ? -seed : seed;
@@ -379,8 +477,8 @@ struct WarpChain {
             ux0 = (uint32_t)(777755555 ^ s);
             seed = s + 1;
         }
-        const int c = (n + 31) / 32;
-        const int k0 = lane * c;
+        const int c = (n + TT - 1) / TT;
+        const int k0 = tid * c;
         const int k1 = min(n, k0 + c);
         uint32_t ux = 0;
         int32_t iy = 0;
@@ -402,22 +500,33 @@ struct WarpChain {
                 S.s0[k] = (double)__fmul_rn(am, __int2float_rn(res));
             }
         }
+        // the state after the last draw, from the thread that made it
         const int last = (n - 1) / c;
-        ux0 = __shfl_sync(kFull, ux, last);
-        iy0 = __shfl_sync(kFull, iy, last);
-        __syncwarp();
+        if constexpr (T == 1) {
+            ux0 = __shfl_sync(kFull, ux, last);
+            iy0 = __shfl_sync(kFull, iy, last);
+            __syncwarp();
+        } else {
+            if (tid == last) {
+                S.bu = ux;
+                S.bi = iy;
+            }
+            sync();
+            ux0 = S.bu;
+            iy0 = S.bi;
+        }
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 double v = 0.0;
                 if (valid(q)) {
-                    const double y = S.s0[3 * (lane + 32 * q) + d] - 0.5;
+                    const double y = S.s0[3 * bead(q) + d] - 0.5;
                     v = (14.14855378 * y * y + 1.21569221) * y;
                 }
                 X[q][d] = (float)v;
             }
-        __syncwarp();
+        sync();
     }
 
     // ---- Lanczos extreme eigenvalues (src/hydrodynamics.cpp:146-264) ----
@@ -426,17 +535,17 @@ struct WarpChain {
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) x[q][d] = valid(q) ? vec[3 * (lane + 32 * q) + d] : 0.0;
+            for (int d = 0; d < 3; ++d) x[q][d] = valid(q) ? vec[3 * bead(q) + d] : 0.0;
     }
     __device__ void store(double* vec, const double (&x)[2][3]) const {
 #pragma unroll
         for (int q = 0; q < 2; ++q)
             if (valid(q))
 #pragma unroll
-                for (int d = 0; d < 3; ++d) vec[3 * (lane + 32 * q) + d] = x[q][d];
+                for (int d = 0; d < 3; ++d) vec[3 * bead(q) + d] = x[q][d];
     }
 
-    // Returns rmin/rmax; writes the Ritz vectors.
+    // Returns the number of Lanczos steps; sets rmin/rmax and the Ritz vectors.
     __device__ int lanczos(int m, bool warm, const double* cache, double (&vmin)[2][3], double (&vmax)[2][3],
                            double& rmin, double& rmax) {
         if (n < m) m = n;
@@ -486,13 +595,10 @@ struct WarpChain {
                             for (int q = 0; q < 2; ++q)
 #pragma unroll
                                 for (int d = 0; d < 3; ++d)
-                                    if (valid(q)) c[u] += w[q][d] * vu[3 * (lane + 32 * q) + d];
+                                    if (valid(q)) c[u] += w[q][d] * vu[3 * bead(q) + d];
                         }
                     }
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                        for (int u = 0; u < kLanczosWarm; ++u) c[u] += __shfl_xor_sync(kFull, c[u], o);
+                    tsum8(c);
 #pragma unroll
                     for (int u = 0; u < kLanczosWarm; ++u) {
                         if (u <= j) {
@@ -501,14 +607,14 @@ struct WarpChain {
                             for (int q = 0; q < 2; ++q)
 #pragma unroll
                                 for (int d = 0; d < 3; ++d)
-                                    if (valid(q)) w[q][d] -= c[u] * vu[3 * (lane + 32 * q) + d];
+                                    if (valid(q)) w[q][d] -= c[u] * vu[3 * bead(q) + d];
                         }
                     }
 #pragma unroll
                     for (int u = 0; u < kLanczosWarm; ++u)
                         if (u == j) al += c[u];
                 }
-                if (lane == 0) S.alpha[k] = al;
+                if (tid == 0) S.alpha[k] = al;
                 ++k;
                 b = sqrt(dot(w, w));
                 if (b < 1.0e-10) break;
@@ -517,69 +623,77 @@ struct WarpChain {
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) v[q][d] = w[q][d] * ib;
-                if (lane == 0) S.beta[j] = b;
+                if (tid == 0) S.beta[j] = b;
             }
         } else {
-        // cold runs (first step of a call): the reference's modified Gram-Schmidt
-        for (int j = 0; j < m; ++j) {
-            store(basis(j, m), v);
-
-            apply(v, w);
-            const double al = dot(v, w);
-            if (lane == 0) S.alpha[k] = al;
-            ++k;
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) w[q][d] -= al * v[q][d] + b * vp[q][d];
-            __syncwarp();
-            for (int u = 0; u <= j; ++u) {
-                double uu[2][3];
-                load(basis(u, m), uu);
-                const double dd = dot(w, uu);
+            // cold runs (first step of a call): the reference's modified Gram-Schmidt
+            for (int j = 0; j < m; ++j) {
+                store(basis(j, m), v);
+                apply(v, w);
+                const double al = dot(v, w);
+                if (tid == 0) S.alpha[k] = al;
+                ++k;
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) w[q][d] -= dd * uu[q][d];
-            }
-            b = sqrt(dot(w, w));
-            if (b < 1.0e-10) break;
-            const double ib = 1.0 / b;
+                    for (int d = 0; d < 3; ++d) w[q][d] -= al * v[q][d] + b * vp[q][d];
+                sync();
+                for (int u = 0; u <= j; ++u) {
+                    double uu[2][3];
+                    load(basis(u, m), uu);
+                    const double dd = dot(w, uu);
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < 2; ++q)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    vp[q][d] = v[q][d];
-                    v[q][d] = w[q][d] * ib;
+                        for (int d = 0; d < 3; ++d) w[q][d] -= dd * uu[q][d];
                 }
-            if (lane == 0) S.beta[j] = b;
+                b = sqrt(dot(w, w));
+                if (b < 1.0e-10) break;
+                const double ib = 1.0 / b;
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        vp[q][d] = v[q][d];
+                        v[q][d] = w[q][d] * ib;
+                    }
+                if (tid == 0) S.beta[j] = b;
+            }
         }
-        }
-        __syncwarp();
+        sync();
         if (k == 1) {
             rmin = rmax = S.alpha[0];
             load(basis(0, m), vmin);
             load(basis(0, m), vmax);
             return 1;
         }
-        double lo = S.alpha[0], hi = S.alpha[0];
-        for (int i = 0; i < k; ++i) {
-            const double rad = (i > 0 ? fabs(S.beta[i - 1]) : 0.0) + (i < k - 1 ? fabs(S.beta[i]) : 0.0);
-            lo = dmin_(lo, S.alpha[i] - rad);
-            hi = dmax_(hi, S.alpha[i] + rad);
+        if (wi == 0) {
+            double lo = S.alpha[0], hi2 = S.alpha[0];
+            for (int i = 0; i < k; ++i) {
+                const double rad = (i > 0 ? fabs(S.beta[i - 1]) : 0.0) + (i < k - 1 ? fabs(S.beta[i]) : 0.0);
+                lo = dmin_(lo, S.alpha[i] - rad);
+                hi2 = dmax_(hi2, S.alpha[i] + rad);
+            }
+            // lanes 0-15 of the first warp bracket the smallest eigenvalue,
+            // lanes 16-31 the largest
+            double l2 = lo, h2 = hi2;
+            halfwarp_bisect(S.alpha, S.beta, k, wl < 16 ? 1 : k, l2, h2);
+            const double r = 0.5 * (l2 + h2);
+            const double r0 = __shfl_sync(kFull, r, 0);
+            const double r1 = __shfl_sync(kFull, r, 16);
+            if (wl == 0 || wl == 16) {
+                const bool lo_end = wl == 0;
+                wk_tridiag_vec(S.alpha, S.beta, k, lo_end ? r0 : r1, lo_end ? S.ymin : S.ymax,
+                               lo_end ? S.s3 : S.s3 + 32, lo_end ? S.s4 : S.s4 + 32);
+            }
+            if (wl == 0) {
+                S.rr[0] = r0;
+                S.rr[1] = r1;
+            }
         }
-        // lanes 0-15 bracket the smallest eigenvalue, lanes 16-31 the largest
-        double l2 = lo, h2 = hi;
-        halfwarp_bisect(S.alpha, S.beta, k, lane < 16 ? 1 : k, l2, h2);
-        const double r = 0.5 * (l2 + h2);
-        rmin = __shfl_sync(kFull, r, 0);
-        rmax = __shfl_sync(kFull, r, 16);
-        if (lane == 0 || lane == 16) {
-            const bool lo_end = lane == 0;
-            wk_tridiag_vec(S.alpha, S.beta, k, lo_end ? rmin : rmax, lo_end ? S.ymin : S.ymax,
-                           lo_end ? S.s3 : S.s3 + 32, lo_end ? S.s4 : S.s4 + 32);
-        }
-        __syncwarp();
+        sync();
+        rmin = S.rr[0];
+        rmax = S.rr[1];
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
@@ -596,7 +710,7 @@ struct WarpChain {
                     vmax[q][d] += y2 * vj[q][d];
                 }
         }
-        __syncwarp();
+        sync();
         return k;
     }
 
@@ -652,19 +766,19 @@ struct WarpChain {
         for (;;) {
             const float inv = 1.f / (float)(L + 1);
             const float ida = 1.f / da;
-            for (int k = lane; k <= L; k += 32) {
+            for (int k = tid; k <= L; k += TT) {
                 const float xk = (cospif(((float)k + 0.5f) * inv) - db) * ida;
                 sqx[k] = sqrtf(xk);
             }
-            __syncwarp();
-            for (int j = lane; j <= L; j += 32) {
+            sync();
+            for (int j = tid; j <= L; j += TT) {
                 float s = 0.f;
                 for (int k = 0; k <= L; ++k) s += sqx[k] * cospif((float)j * ((float)k + 0.5f) * inv);
                 s *= 2.f * inv;
                 if (j == 0) s *= 0.5f;
                 coef[j] = s;
             }
-            __syncwarp();
+            sync();
             float tp[2][3], tc[2][3], o[2][3];
             const float c0 = coef[0], c1 = coef[1];
 #pragma unroll
@@ -696,7 +810,7 @@ struct WarpChain {
                 for (int d = 0; d < 3; ++d) out[q][d] = valid(q) ? o[q][d] : 0.f;
             const double rr = dotf(out, out);
             fd = fabs(rr - x0Dx0) / x0Dx0;
-            __syncwarp();
+            sync();
             if (fd <= ch.fd_tol || L >= kMaxCheb) break;
             const int grow = L / 4 > 1 ? L / 4 : 1;
             L = (L + grow) > kMaxCheb ? kMaxCheb : L + grow;
@@ -708,14 +822,14 @@ struct WarpChain {
     // scratch, right-looking factor, L x0. Returns false if not PD.
     __device__ bool cholesky_noise(const double (&R)[2][3], const float (&x0)[2][3], float (&out)[2][3]) {
         to_smem(S.s0, R);
-        __syncwarp();
+        sync();
         double* L = Lt;
-        for (int idx = lane; idx < 9 * N; idx += 32) {
+        for (int idx = tid; idx < 9 * N; idx += TT) {
             const int mu = idx / 9, i = (idx % 9) / 3, j = idx % 3;
             L[(int64_t)(3 * mu + i) * n + 3 * mu + j] = (i == j) ? 1.0 : 0.0;
         }
         const int npairs = N * (N - 1) / 2;
-        for (int pidx = lane; pidx < npairs; pidx += 32) {
+        for (int pidx = tid; pidx < npairs; pidx += TT) {
             int nu = (int)((1.0 + sqrt(1.0 + 8.0 * (double)pidx)) * 0.5);
             while (nu * (nu - 1) / 2 > pidx) --nu;
             while ((nu + 1) * nu / 2 <= pidx) ++nu;
@@ -731,84 +845,96 @@ struct WarpChain {
                     L[(int64_t)(3 * nu + j) * n + 3 * mu + i] = val;
                 }
         }
-        __syncwarp();
+        __threadfence_block();
+        sync();
         for (int k = 0; k < n; ++k) {
             const double s = L[(int64_t)k * n + k];
             if (!(s > 0.0)) return false;
             const double dk = sqrt(s);
-            __syncwarp();
-            if (lane == 0) L[(int64_t)k * n + k] = dk;
+            sync();
+            if (tid == 0) L[(int64_t)k * n + k] = dk;
             const double idk = 1.0 / dk;
-            for (int i = k + 1 + lane; i < n; i += 32) L[(int64_t)k * n + i] *= idk;
-            __syncwarp();
+            for (int i = k + 1 + tid; i < n; i += TT) L[(int64_t)k * n + i] *= idk;
+            __threadfence_block();
+            sync();
             const double* colk = L + (int64_t)k * n;
             for (int j = k + 1; j < n; ++j) {
                 const double ljk = colk[j];
-                for (int i = j + lane; i < n; i += 32) L[(int64_t)j * n + i] -= colk[i] * ljk;
+                for (int i = j + tid; i < n; i += TT) L[(int64_t)j * n + i] -= colk[i] * ljk;
             }
-            __syncwarp();
+            __threadfence_block();
+            sync();
         }
 #pragma unroll
         for (int q = 0; q < 2; ++q)
             if (valid(q))
 #pragma unroll
-                for (int d = 0; d < 3; ++d) S.s1[3 * (lane + 32 * q) + d] = (double)x0[q][d];
-        __syncwarp();
+                for (int d = 0; d < 3; ++d) S.s1[3 * bead(q) + d] = (double)x0[q][d];
+        sync();
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                const int i = 3 * (lane + 32 * q) + d;
+                const int i = 3 * bead(q) + d;
                 double s = 0.0;
                 if (valid(q))
                     for (int j = 0; j <= i; ++j) s += L[(int64_t)j * n + i] * S.s1[j];
                 out[q][d] = (float)s;
             }
-        __syncwarp();
+        sync();
         return true;
     }
 };
 
 // -------------------------------------------------------------- the kernel
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(const RunArgs a) {
+template <int T>
+__global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlocks)
+    integrate_team_kernel(const RunArgs a) {
     extern __shared__ __align__(16) unsigned char wsm[];
-    const int warp = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
-    const int64_t stride = warp_smem_stride(a.n_max);
-    WarpShared& S = *reinterpret_cast<WarpShared*>(wsm + stride * warp);
-    double* Vs = reinterpret_cast<double*>(wsm + stride * warp + (sizeof(WarpShared) + 15) / 16 * 16);
-    const int64_t gw = (int64_t)blockIdx.x * kWarpsPerCta + warp;
+    constexpr int TT = TeamCfg<T>::kThreads;
+    const int team = threadIdx.x / TT;
+    const int tid = threadIdx.x % TT;
+    const int64_t stride = team_area_stride<T>(a.n_max);
+    TeamShared<T>& S = *reinterpret_cast<TeamShared<T>*>(wsm + stride * team);
+    double* Vs = reinterpret_cast<double*>(wsm + stride * team + (sizeof(TeamShared<T>) + 15) / 16 * 16);
+    const int64_t gw = (int64_t)blockIdx.x * TeamCfg<T>::kTeamsPerCta + team;
     double* scr = a.scratch + gw * a.scratch_stride;
     const int nvr = (int)round_up8(a.n_max);
 
     for (;;) {
-        int c = 0;
-        if (lane == 0) c = atomicAdd(a.work_counter, 1);
-        c = __shfl_sync(kFull, c, 0);
-        if (c >= a.n_chains) break;
+        if (tid == 0) {
+            const int item = atomicAdd(a.work_counter, 1);
+            S.item = item >= a.n_work ? -1 : (a.order ? a.order[item] : item);
+        }
+        team_sync<T>(team);
+        const int c = S.item;
+        if (c < 0) break;
         {
             const int nw = (int)(sizeof(DevChain) / 8);
             const double* src = reinterpret_cast<const double*>(a.chains + c);
             double* dst = reinterpret_cast<double*>(&S.ch);
-            for (int i = lane; i < nw; i += 32) dst[i] = src[i];
+            for (int i = tid; i < nw; i += TT) dst[i] = src[i];
         }
-        __syncwarp();
+        team_sync<T>(team);
         const DevChain& ch = S.ch;
         int status = a.status[c];
         if ((status & BDCU_ST_FATAL_MASK) || ch.bad_param) {
-            if (lane == 0 && ch.bad_param) a.status[c] = status | BDCU_ST_BAD_PARAM;
-            __syncwarp();
+            if (tid == 0 && ch.bad_param) a.status[c] = status | BDCU_ST_BAD_PARAM;
+            team_sync<T>(team);
             continue;
         }
-        WarpChain W(a, S, ch);
+        TeamChain<T> W(a, S, ch);
         W.V = Vs;
         W.sqx = reinterpret_cast<float*>(Vs);
         W.coef = reinterpret_cast<float*>(Vs) + kCoefCap;
         W.Vg = scr;
         W.Lt = scr + (int64_t)kLanczosCold * nvr;
         W.nv = nvr;
-        W.lane = lane;
+        W.tid = tid;
+        W.wl = tid & 31;
+        W.wi = tid >> 5;
+        W.team = team;
         W.N = ch.N;
         W.n = 3 * ch.N;
         W.hi = ch.hstar > 0.0;
@@ -846,7 +972,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                     double s = 0.0;
 #pragma unroll
                     for (int q = 0; q < 2; ++q) s += R[q][d];
-                    com[d] = (1.0 / N) * wsum(s);
+                    com[d] = (1.0 / N) * W.tsum(s);
                 }
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
@@ -922,14 +1048,14 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                     ups[q][r] = R[q][r] + dt * (0.5 * (fl1 + fl2) + 0.125 * DFs[q][r] + 0.125 * DFe[q][r]) +
                                 sqrt2inv * dW[q][r];
                 }
-            // solve_connectors (src/integrator.cpp:125-165): lane owns bonds lane, lane+32
+            // solve_connectors (src/integrator.cpp:125-165): thread owns bonds bead(0), bead(1)
             W.to_smem(S.s0, ups);
             W.to_smem(S.s1, Rp);
-            __syncwarp();
+            team_sync<T>(team);
             double dups[2][3], bond[2][3];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                const int b = lane + 32 * q;
+                const int b = W.bead(q);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const bool ok = b < N - 1;
@@ -938,7 +1064,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                 }
             }
             const double anchor0 = S.s1[0], anchor1 = S.s1[1], anchor2 = S.s1[2];
-            __syncwarp();
+            team_sync<T>(team);
             double Rprev[2][3], Rc[2][3];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
@@ -952,7 +1078,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                 double Fc[2][3];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    const int b = lane + 32 * q;
+                    const int b = W.bead(q);
                     const double f =
                         b < N - 1 ? connector_factor(ch, clamped_len(bond[q][0], bond[q][1], bond[q][2])) : 0.0;
 #pragma unroll
@@ -961,11 +1087,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                         if (b < N - 1) S.s1[3 * b + d] = Fc[q][d];
                     }
                 }
-                __syncwarp();
+                team_sync<T>(team);
                 float Fb[2][3], DFb[2][3];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    const int m = lane + 32 * q;
+                    const int m = W.bead(q);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         double v = 0.0;
@@ -977,17 +1103,17 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                         Fb[q][d] = (float)v;
                     }
                 }
-                __syncwarp();
+                team_sync<T>(team);
                 W.applyF(Fb, DFb);
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
                     if (W.valid(q))
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) S.s2[3 * (lane + 32 * q) + d] = (double)DFb[q][d];
-                __syncwarp();
+                        for (int d = 0; d < 3; ++d) S.s2[3 * W.bead(q) + d] = (double)DFb[q][d];
+                team_sync<T>(team);
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    const int b = lane + 32 * q;
+                    const int b = W.bead(q);
                     if (b < N - 1) {
                         double g[3], qv[3];
                         for (int d = 0; d < 3; ++d)
@@ -996,7 +1122,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                         for (int d = 0; d < 3; ++d) bond[q][d] = qv[d];
                     }
                 }
-                // R_corr = anchor + prefix sums of the bonds (warp scan, two segments)
+                // R_corr = anchor + prefix sums of the bonds: inclusive scan in
+                // each warp, then the totals of the warps before it (slot 0 of
+                // the whole team precedes slot 1)
                 double scan[2][3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -1005,17 +1133,43 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                     for (int o = 1; o < 32; o <<= 1) {
                         const double t0 = __shfl_up_sync(kFull, v0, o);
                         const double t1 = __shfl_up_sync(kFull, v1, o);
-                        if (lane >= o) {
+                        if (W.wl >= o) {
                             v0 += t0;
                             v1 += t1;
                         }
                     }
-                    const double carry = __shfl_sync(kFull, v0, 31);
                     scan[0][d] = v0;
-                    scan[1][d] = v1 + carry;
+                    scan[1][d] = v1;
                 }
-                __syncwarp();
-                if (lane == 0) {
+                if constexpr (T == 1) {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) scan[1][d] += __shfl_sync(kFull, scan[0][d], 31);
+                    __syncwarp();
+                } else {
+                    if (W.wl == 31)
+#pragma unroll
+                        for (int q = 0; q < 2; ++q)
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) S.tot[(q * 3 + d) * T + W.wi] = scan[q][d];
+                    team_sync<T>(team);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        double off0 = 0.0, all0 = 0.0, off1 = 0.0;
+#pragma unroll
+                        for (int w = 0; w < T; ++w) {
+                            const double t0 = S.tot[d * T + w], t1 = S.tot[(3 + d) * T + w];
+                            if (w < W.wi) {
+                                off0 += t0;
+                                off1 += t1;
+                            }
+                            all0 += t0;
+                        }
+                        scan[0][d] += off0;
+                        scan[1][d] += all0 + off1;
+                    }
+                }
+                team_sync<T>(team);
+                if (tid == 0) {
                     S.s1[0] = anchor0;
                     S.s1[1] = anchor1;
                     S.s1[2] = anchor2;
@@ -1023,13 +1177,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                 const double an[3] = {anchor0, anchor1, anchor2};
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
-                    const int b = lane + 32 * q;
+                    const int b = W.bead(q);
                     if (b < N - 1)
                         for (int d = 0; d < 3; ++d) S.s1[3 * (b + 1) + d] = an[d] + scan[q][d];
                 }
-                __syncwarp();
+                team_sync<T>(team);
                 W.load(S.s1, Rc);
-                __syncwarp();
+                team_sync<T>(team);
                 double s = 0.0;
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
@@ -1038,7 +1192,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
                                      e2 = Rc[q][2] - Rprev[q][2];
                         s += e0 * e0 + e1 * e1 + e2 * e2;
                     }
-                const double incr = sqrt(wsum(s)) / N;
+                const double incr = sqrt(W.tsum(s)) / N;
                 W.cnt[C_CORR] += 1;
                 if (incr < ch.tol) break;
                 if (!(incr == incr) || isinf(incr)) {
@@ -1055,8 +1209,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
 #pragma unroll
                     for (int d = 0; d < 3; ++d) Rprev[q][d] = Rc[q][d];
             }
-            // every lane's connector status, then a warp-uniform fatal test
-            W.status |= __reduce_or_sync(kFull, lstat);
+            // every thread's connector status, then a team-uniform fatal test
+            W.status |= W.tor(lstat);
             if (W.status & BDCU_ST_FATAL_MASK) break;
 #pragma unroll
             for (int q = 0; q < 2; ++q)
@@ -1066,7 +1220,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
             t += dt;
         }
         if (!(W.status & BDCU_ST_FATAL_MASK)) W.store(gR, R);
-        if (lane == 0) {
+        if (tid == 0) {
             a.rng[3 * c] = (int32_t)ux;
             a.rng[3 * c + 1] = iy;
             a.rng[3 * c + 2] = seed;
@@ -1075,7 +1229,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, 2) integrate_warp_kernel(co
             int64_t* cc = reinterpret_cast<int64_t*>(a.counters + c);
             for (int k = 0; k < 8; ++k) cc[k] += W.cnt[k];
         }
-        __syncwarp();
+        team_sync<T>(team);
     }
 }
 

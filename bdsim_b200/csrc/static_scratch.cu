@@ -4,10 +4,11 @@
 // Some callers cannot call cudaMalloc: a host application whose memory pool
 // already owns all of the GPU's memory, or a serving loop that must never take
 // the implicit device-wide synchronisation cudaMalloc/cudaFree imply. For them
-// this entry point runs the same integrator kernel as bdcu_run, but every
-// device buffer it needs beyond the caller's inputs and outputs -- the chain
-// parameter records, the parameter arena, the Lanczos seed table, the work
-// queue counter and the per-block scratch -- lives in one file-scope
+// this entry point runs the same kernels as bdcu_run, bucket by bucket, but
+// every device buffer it needs beyond the caller's inputs and outputs -- the
+// chain parameter records, the work lists, the parameter arena, the Lanczos
+// seed table, the RNG jump-ahead tables, the work queue counters and the
+// per-block scratch -- lives in one file-scope
 // `static __device__` array of kStaticScratchBytes. Every GPU that loads the
 // library holds that array until the process exits.
 //
@@ -15,7 +16,7 @@
 // taken once per device with cudaGetSymbolAddress (the first call on a device
 // does it; make that first call before any stream capture on the device).
 // Every call shares the array and it keeps the last call's contents: the work
-// counter is cleared on each call, and everything else is written before it
+// counters are cleared on each call, and everything else is written before it
 // is read. Calls that overlap on the GPU (two streams, two host threads) race
 // on the array and must be serialised by the caller.
 #include <cuda_runtime.h>
@@ -29,15 +30,16 @@
 
 #include "ctx.h"
 #include "integrator.cuh"
-#include "warp_layout.h"
+#include "plan.h"
+#include "team_layout.h"
 
 namespace bdcu {
 cudaError_t launch_plain(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t launch_mixed(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t occupancy_plain(int block, size_t smem, int* per_sm);
 cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm);
-cudaError_t launch_mixed_warp(const RunArgs& a, int grid, size_t smem, cudaStream_t s);
-cudaError_t occupancy_mixed_warp(size_t smem, int* per_sm);
+cudaError_t launch_mixed_team(int team_warps, const RunArgs& a, int grid, size_t smem, cudaStream_t s);
+cudaError_t occupancy_mixed_team(int team_warps, size_t smem, int* per_sm);
 DevChain derive_record(const bdcu_phys& p, const bdcu_sim& s, int64_t bead_off);
 }  // namespace bdcu
 
@@ -72,91 +74,6 @@ int fail(bdcu_ctx* c, int code, const std::string& msg) {
     return code;
 }
 
-// The one-chain-per-warp mixed form, as bdcu_run dispatches it; the RNG
-// jump-ahead rows k = 0..n_max it reads are staged into the array too.
-int run_static_warp(bdcu_ctx* ctx, int n_chains, const std::vector<DevChain>& recs, const std::vector<double>& seed,
-                    const double* arena, int64_t arena_len, int n_max, int any_hi, int any_cheb, double* R,
-                    int32_t* rng, double* cache, int32_t* cache_valid, const double* t_start,
-                    const int32_t* n_steps, int32_t* status, bdcu_counters* counters, int cache_mode) {
-    const size_t smem = (size_t)warp_smem_bytes(n_max);
-    if (smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: warp kernel shared memory too large");
-    int per_sm = 0;
-    cudaError_t e = occupancy_mixed_warp(smem, &per_sm);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
-    if (per_sm < 1) per_sm = 1;
-    std::vector<uint32_t> cols((size_t)(n_max + 1) * 32);
-    std::vector<uint32_t> apow(n_max + 1);
-    for (int i = 0; i < 32; ++i) cols[i] = 1u << i;
-    apow[0] = 1;
-    for (int k = 1; k <= n_max; ++k) {
-        for (int i = 0; i < 32; ++i) {
-            uint32_t u = cols[(size_t)(k - 1) * 32 + i];
-            u ^= (u << 13);
-            u ^= (u >> 17);
-            u ^= (u << 5);
-            cols[(size_t)k * 32 + i] = u;
-        }
-        apow[k] = (uint32_t)(((uint64_t)apow[k - 1] * 16807ull) % 2147483647ull);
-    }
-    const size_t o_cnt = 0;
-    const size_t o_rec = 256;
-    const size_t o_seed = align256(o_rec + sizeof(DevChain) * (size_t)n_chains);
-    const size_t o_arena = align256(o_seed + sizeof(double) * (size_t)n_max);
-    const size_t o_cols = align256(o_arena + sizeof(double) * (size_t)std::max<int64_t>(arena_len, 1));
-    const size_t o_apow = align256(o_cols + sizeof(uint32_t) * cols.size());
-    const size_t o_scr = align256(o_apow + sizeof(uint32_t) * apow.size());
-    const int64_t wstride = any_hi ? warp_scratch_doubles(n_max) : 1;
-    const size_t per_block = sizeof(double) * (size_t)wstride * kWarpsPerCta;
-    if (o_scr + per_block > kStaticScratchBytes)
-        return fail(ctx, BDCU_E_LIMIT,
-                    "bdcu_run_static: needs " + std::to_string(o_scr + per_block) + " bytes of static device scratch "
-                    "for this batch (parameters plus one block's scratch); the maximum is " +
-                    std::to_string(kStaticScratchBytes) + " bytes. Use bdcu_run, or fewer/smaller chains.");
-    int grid = std::min((n_chains + kWarpsPerCta - 1) / kWarpsPerCta, per_sm * ctx->sm_count);
-    grid = (int)std::min<size_t>((size_t)grid, (kStaticScratchBytes - o_scr) / per_block);
-    if (grid < 1) grid = 1;
-    void* base = nullptr;
-    e = static_base(ctx->device, &base);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    unsigned char* b = static_cast<unsigned char*>(base);
-    cudaStream_t s = ctx->stream;
-    e = cudaMemsetAsync(b + o_cnt, 0, sizeof(int32_t), s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_rec, recs.data(), sizeof(DevChain) * n_chains, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_seed, seed.data(), sizeof(double) * n_max, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && arena_len > 0)
-        e = cudaMemcpyAsync(b + o_arena, arena, sizeof(double) * arena_len, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_cols, cols.data(), sizeof(uint32_t) * cols.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_apow, apow.data(), sizeof(uint32_t) * apow.size(), cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("staging parameters: ") + cudaGetErrorString(e));
-    RunArgs a;
-    memset(&a, 0, sizeof(a));
-    a.chains = reinterpret_cast<const DevChain*>(b + o_rec);
-    a.n_chains = n_chains;
-    a.n_max = n_max;
-    a.arena = reinterpret_cast<const double*>(b + o_arena);
-    a.seed_table = reinterpret_cast<const double*>(b + o_seed);
-    a.R = R;
-    a.rng = rng;
-    a.cache = cache;
-    a.cache_valid = cache_valid;
-    a.t_start = t_start;
-    a.n_steps = n_steps;
-    a.status = status;
-    a.counters = counters;
-    a.cache_mode = cache_mode;
-    a.need_chol = any_hi;
-    a.need_d = any_hi;
-    a.need_lz = any_cheb;
-    a.work_counter = reinterpret_cast<int32_t*>(b + o_cnt);
-    a.scratch = reinterpret_cast<double*>(b + o_scr);
-    a.scratch_stride = wstride;
-    a.xs_pow = reinterpret_cast<const uint32_t*>(b + o_cols);
-    a.a_pow = reinterpret_cast<const uint32_t*>(b + o_apow);
-    e = launch_mixed_warp(a, grid, smem, s);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("integrate kernel launch: ") + cudaGetErrorString(e));
-    return BDCU_OK;
-}
-
 }  // namespace
 
 extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bdcu_sim* sim,
@@ -177,7 +94,7 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
     // chain records, derived on the host exactly as bdcu_set_chains derives them
     std::vector<DevChain> recs(n_chains);
     int64_t off = 0;
-    int n_max = 0, any_hi = 0, any_cheb = 0;
+    int n_max = 0;
     for (int i = 0; i < n_chains; ++i) {
         const bdcu_phys& p = phys[i];
         if (p.n_beads < 2 || p.n_beads > kMaxBeads || !(sim[i].dt > 0.0))
@@ -192,101 +109,170 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
         recs[i] = derive_record(p, sim[i], off);
         off += p.n_beads;
         n_max = std::max(n_max, 3 * p.n_beads);
-        if (p.hstar > 0.0) {
-            any_hi = 1;
-            if (p.hi_method == BDCU_HI_CHEBYSHEV) any_cheb = 1;
-        }
     }
     std::vector<double> seed(n_max);
     for (int i = 0; i < n_max; ++i) seed[i] = sin(0.7654321 * (i + 1)) + 0.5;
 
-    int any_chol_method = 0;
-    for (int i = 0; i < n_chains; ++i)
-        if (phys[i].hstar > 0.0 && phys[i].hi_method == BDCU_HI_CHOLESKY) any_chol_method = 1;
-    if (form == BDCU_FORM_MIXED_FP32 && n_max <= kWarpMaxn && !any_chol_method)
-        return run_static_warp(ctx, n_chains, recs, seed, arena, arena_len, n_max, any_hi, any_cheb, R, rng, cache,
-                               cache_valid, t_start, n_steps, status, counters, cache_mode);
-
-    // launch shape, as bdcu_run plans it
+    // buckets, as bdcu_run plans them (largest chains first within a bucket)
     const int mixed = (form == BDCU_FORM_MIXED_FP32);
-    std::vector<int> d_opts = (!mixed && any_hi) ? std::vector<int>{1, 0} : std::vector<int>{0};
-    std::vector<int> v_opts = any_cheb ? std::vector<int>{kLanczosCold, kLanczosWarm, 0} : std::vector<int>{0};
-    int dsm = -1, vcap = 0;
-    size_t smem = 0;
-    for (int d : d_opts) {
-        for (int v : v_opts) {
-            const size_t b = (size_t)smem_layout(n_max, d, v, mixed).total * sizeof(double);
-            if (b <= ctx->max_smem) {
-                dsm = d;
-                vcap = v;
-                smem = b;
-                break;
+    std::vector<std::vector<int32_t>> lists(kMaxBuckets);
+    for (int i = 0; i < n_chains; ++i) lists[bucket_of(recs[i], form)].push_back(i);
+    struct Launch {
+        int id, team_warps, block, grid, v_cap, d_in_smem, n_max, need_d, need_lz, count;
+        size_t smem, per_block;
+        int64_t stride, order_off;
+    };
+    std::vector<Launch> launches;
+    std::vector<int32_t> order;
+    bool any_team = false;
+    size_t max_block_scratch = 0;
+    for (int id = kMaxBuckets - 1; id >= 0; --id) {
+        std::vector<int32_t>& L = lists[id];
+        if (L.empty()) continue;
+        std::stable_sort(L.begin(), L.end(), [&](int32_t x, int32_t y) { return recs[x].N > recs[y].N; });
+        Launch l;
+        memset(&l, 0, sizeof(l));
+        l.id = id;
+        l.count = (int)L.size();
+        l.n_max = 3 * recs[L.front()].N;
+        for (int32_t c : L)
+            if (recs[c].hstar > 0.0) {
+                l.need_d = 1;
+                if (recs[c].hi_method == BDCU_HI_CHEBYSHEV) l.need_lz = 1;
             }
+        l.order_off = (int64_t)order.size();
+        order.insert(order.end(), L.begin(), L.end());
+        int per_sm = 0;
+        if (id < kFirstBlockBucket) {
+            any_team = true;
+            l.team_warps = 1 << id;
+            l.smem = (size_t)team_smem(l.team_warps, l.n_max);
+            if (l.smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: team kernel shared memory too large");
+            e = occupancy_mixed_team(l.team_warps, l.smem, &per_sm);
+            l.stride = l.need_d ? team_scratch_doubles(l.n_max) : 1;
+            l.per_block = sizeof(double) * (size_t)l.stride * teams_per_cta(l.team_warps);
+            l.block = 32 * l.team_warps * teams_per_cta(l.team_warps);
+            l.grid = (l.count + teams_per_cta(l.team_warps) - 1) / teams_per_cta(l.team_warps);
+        } else {
+            std::vector<int> d_opts = (!mixed && l.need_d) ? std::vector<int>{1, 0} : std::vector<int>{0};
+            std::vector<int> v_opts = l.need_lz ? std::vector<int>{kLanczosCold, kLanczosWarm, 0} : std::vector<int>{0};
+            l.d_in_smem = -1;
+            for (int d : d_opts) {
+                for (int v : v_opts) {
+                    const size_t bytes = (size_t)smem_layout(l.n_max, d, v, mixed).total * sizeof(double);
+                    if (bytes <= ctx->max_smem) {
+                        l.d_in_smem = d;
+                        l.v_cap = v;
+                        l.smem = bytes;
+                        break;
+                    }
+                }
+                if (l.d_in_smem >= 0) break;
+            }
+            if (l.d_in_smem < 0) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: chain too large for the shared-memory layout");
+            l.block = widest_block(l.n_max);
+            const ScratchLayout scl = scratch_layout(l.n_max, l.d_in_smem, l.v_cap, l.need_d, mixed, l.need_d, l.need_lz);
+            l.stride = std::max<int64_t>(scl.total, 1);
+            l.per_block = sizeof(double) * (size_t)l.stride;
+            e = mixed ? occupancy_mixed(l.block, l.smem, &per_sm) : occupancy_plain(l.block, l.smem, &per_sm);
+            l.grid = l.count;
         }
-        if (dsm >= 0) break;
+        if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
+        if (per_sm < 1) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: kernel shape cannot be resident");
+        l.grid = std::max(1, std::min(l.grid, per_sm * ctx->sm_count));
+        max_block_scratch = std::max(max_block_scratch, l.per_block);
+        launches.push_back(l);
     }
-    if (dsm < 0) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: chain too large for the shared-memory layout");
-    int block = ((std::min(n_max, 512) + 31) / 32) * 32;
-    if (block < 64) block = 64;
-    const ScratchLayout scl = scratch_layout(n_max, dsm, vcap, any_hi, mixed, any_hi, any_cheb);
-    int per_sm = 0;
-    e = mixed ? occupancy_mixed(block, smem, &per_sm) : occupancy_plain(block, smem, &per_sm);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("occupancy query: ") + cudaGetErrorString(e));
-    if (per_sm < 1) per_sm = 1;
 
-    // layout of the static array: counter | records | seed table | arena | per-block scratch
+    // RNG jump-ahead rows k = 0..n_max for the team kernel's noise
+    std::vector<uint32_t> cols, apow;
+    if (any_team) {
+        cols.resize((size_t)(n_max + 1) * 32);
+        apow.resize(n_max + 1);
+        for (int i = 0; i < 32; ++i) cols[i] = 1u << i;
+        apow[0] = 1;
+        for (int k = 1; k <= n_max; ++k) {
+            for (int i = 0; i < 32; ++i) {
+                uint32_t u = cols[(size_t)(k - 1) * 32 + i];
+                u ^= (u << 13);
+                u ^= (u >> 17);
+                u ^= (u << 5);
+                cols[(size_t)k * 32 + i] = u;
+            }
+            apow[k] = (uint32_t)(((uint64_t)apow[k - 1] * 16807ull) % 2147483647ull);
+        }
+    }
+
+    // layout of the static array: queue counters | records | work lists | seed
+    // table | arena | jump-ahead tables | scratch (reused by each bucket in turn)
     const size_t o_cnt = 0;
     const size_t o_rec = 256;
-    const size_t o_seed = align256(o_rec + sizeof(DevChain) * (size_t)n_chains);
+    const size_t o_ord = align256(o_rec + sizeof(DevChain) * (size_t)n_chains);
+    const size_t o_seed = align256(o_ord + sizeof(int32_t) * order.size());
     const size_t o_arena = align256(o_seed + sizeof(double) * (size_t)n_max);
-    const size_t o_scr = align256(o_arena + sizeof(double) * (size_t)std::max<int64_t>(arena_len, 1));
-    const size_t stride = sizeof(double) * (size_t)std::max<int64_t>(scl.total, 1);
-    if (o_scr + stride > kStaticScratchBytes)
+    const size_t o_cols = align256(o_arena + sizeof(double) * (size_t)std::max<int64_t>(arena_len, 1));
+    const size_t o_apow = align256(o_cols + sizeof(uint32_t) * cols.size());
+    const size_t o_scr = align256(o_apow + sizeof(uint32_t) * apow.size());
+    if (o_scr + max_block_scratch > kStaticScratchBytes)
         return fail(ctx, BDCU_E_LIMIT,
-                    "bdcu_run_static: needs " + std::to_string(o_scr + stride) + " bytes of static device scratch "
-                    "for this batch (parameters plus one block's scratch); the maximum is " +
-                    std::to_string(kStaticScratchBytes) + " bytes. Use bdcu_run, or fewer/smaller chains.");
-    int grid = std::min(n_chains, per_sm * ctx->sm_count);
-    grid = (int)std::min<size_t>((size_t)grid, (kStaticScratchBytes - o_scr) / stride);
-    if (grid < 1) grid = 1;
+                    "bdcu_run_static: needs " + std::to_string(o_scr + max_block_scratch) +
+                    " bytes of static device scratch for this batch (parameters plus one block's scratch); the "
+                    "maximum is " + std::to_string(kStaticScratchBytes) + " bytes. Use bdcu_run, or fewer/smaller chains.");
+    for (Launch& l : launches)
+        l.grid = (int)std::max<size_t>(1, std::min<size_t>((size_t)l.grid, (kStaticScratchBytes - o_scr) / l.per_block));
 
     void* base = nullptr;
     e = static_base(ctx->device, &base);
     if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     unsigned char* b = static_cast<unsigned char*>(base);
     cudaStream_t s = ctx->stream;
-    e = cudaMemsetAsync(b + o_cnt, 0, sizeof(int32_t), s);
+    e = cudaMemsetAsync(b + o_cnt, 0, sizeof(int32_t) * kMaxBuckets, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_rec, recs.data(), sizeof(DevChain) * n_chains, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_ord, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b + o_seed, seed.data(), sizeof(double) * n_max, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && arena_len > 0)
         e = cudaMemcpyAsync(b + o_arena, arena, sizeof(double) * arena_len, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && any_team)
+        e = cudaMemcpyAsync(b + o_cols, cols.data(), sizeof(uint32_t) * cols.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && any_team)
+        e = cudaMemcpyAsync(b + o_apow, apow.data(), sizeof(uint32_t) * apow.size(), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("staging parameters: ") + cudaGetErrorString(e));
 
-    RunArgs a;
-    memset(&a, 0, sizeof(a));
-    a.chains = reinterpret_cast<const DevChain*>(b + o_rec);
-    a.n_chains = n_chains;
-    a.n_max = n_max;
-    a.arena = reinterpret_cast<const double*>(b + o_arena);
-    a.seed_table = reinterpret_cast<const double*>(b + o_seed);
-    a.R = R;
-    a.rng = rng;
-    a.cache = cache;
-    a.cache_valid = cache_valid;
-    a.t_start = t_start;
-    a.n_steps = n_steps;
-    a.status = status;
-    a.counters = counters;
-    a.cache_mode = cache_mode;
-    a.d_in_smem = dsm;
-    a.v_cap = vcap;
-    a.need_chol = any_hi;
-    a.need_d = any_hi;
-    a.need_lz = any_cheb;
-    a.work_counter = reinterpret_cast<int32_t*>(b + o_cnt);
-    a.scratch = reinterpret_cast<double*>(b + o_scr);
-    a.scratch_stride = std::max<int64_t>(scl.total, 1);
-    e = mixed ? launch_mixed(a, grid, block, smem, s) : launch_plain(a, grid, block, smem, s);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("integrate kernel launch: ") + cudaGetErrorString(e));
+    for (const Launch& l : launches) {
+        RunArgs a;
+        memset(&a, 0, sizeof(a));
+        a.chains = reinterpret_cast<const DevChain*>(b + o_rec);
+        a.n_chains = n_chains;
+        a.order = reinterpret_cast<const int32_t*>(b + o_ord) + l.order_off;
+        a.n_work = l.count;
+        a.n_max = l.n_max;
+        a.arena = reinterpret_cast<const double*>(b + o_arena);
+        a.seed_table = reinterpret_cast<const double*>(b + o_seed);
+        a.R = R;
+        a.rng = rng;
+        a.cache = cache;
+        a.cache_valid = cache_valid;
+        a.t_start = t_start;
+        a.n_steps = n_steps;
+        a.status = status;
+        a.counters = counters;
+        a.cache_mode = cache_mode;
+        a.d_in_smem = l.d_in_smem;
+        a.v_cap = l.v_cap;
+        a.need_chol = l.need_d;
+        a.need_d = l.need_d;
+        a.need_lz = l.need_lz;
+        a.work_counter = reinterpret_cast<int32_t*>(b + o_cnt) + l.id;
+        a.scratch = reinterpret_cast<double*>(b + o_scr);
+        a.scratch_stride = l.stride;
+        a.xs_pow = reinterpret_cast<const uint32_t*>(b + o_cols);
+        a.a_pow = reinterpret_cast<const uint32_t*>(b + o_apow);
+        if (l.id < kFirstBlockBucket)
+            e = launch_mixed_team(l.team_warps, a, l.grid, l.smem, s);
+        else
+            e = mixed ? launch_mixed(a, l.grid, l.block, l.smem, s) : launch_plain(a, l.grid, l.block, l.smem, s);
+        if (e != cudaSuccess)
+            return fail(ctx, BDCU_E_CUDA, std::string("integrate kernel launch: ") + cudaGetErrorString(e));
+    }
     return BDCU_OK;
 }

@@ -111,6 +111,98 @@ class Context:
         self.use_stream()
         self._ck(self.lib.bdcu_forces(self.h, dptr(R_dev), float(t), int(which), dptr(F_dev)), "bdcu_forces")
 
+    # ---- launch plans (buckets by bead count, autotuned shapes)
+
+    def describe_plan(self, form) -> list:
+        """The buckets bdcu_run would launch for `form` on the current selection."""
+        out = (_abi.BdcuBucketInfo * _abi.MAX_BUCKETS)()
+        n = ctypes.c_int(0)
+        self._ck(self.lib.bdcu_describe_plan(self.h, form_code(form), out, _abi.MAX_BUCKETS, ctypes.byref(n)),
+                 "bdcu_describe_plan")
+        return [out[i].as_dict() for i in range(n.value)]
+
+    def autotune(self, form, R, rng, cache, cache_valid, t_start, probe_steps: int = 3) -> list:
+        """Time the block-kernel launch shapes of each bucket on copies of the
+        given state and keep the fastest; returns the tuned plan."""
+        self.use_stream()
+        self._ck(self.lib.bdcu_autotune(self.h, form_code(form), dptr(R), dptr(rng), dptr(cache),
+                                        dptr(cache_valid), dptr(t_start), int(probe_steps)), "bdcu_autotune")
+        return self.describe_plan(form)
+
+    # ---- slot pools (serving)
+
+    def reserve(self, n_slots: int, bead_capacity: int, arena_len: int = 0):
+        self.use_stream()
+        self._ck(self.lib.bdcu_reserve(self.h, int(n_slots), int(bead_capacity), int(arena_len)), "bdcu_reserve")
+        self.n_chains = int(n_slots)
+
+    def update_chains(self, slots, phys_recs, sim_recs, bead_offs):
+        """Fill pool slots: `phys_recs`/`sim_recs` are ctypes arrays of
+        BdcuPhys/BdcuSim (offsets into the context arena already set)."""
+        self.use_stream()
+        slots = np.ascontiguousarray(slots, dtype=np.int32)
+        offs = np.ascontiguousarray(bead_offs, dtype=np.int64)
+        self._ck(self.lib.bdcu_update_chains(self.h, len(slots), slots.ctypes.data_as(_abi.c_int32_p), phys_recs,
+                                             sim_recs, offs.ctypes.data_as(_abi.c_int64_p)), "bdcu_update_chains")
+
+    @staticmethod
+    def pack_slots(phys_list, sim_list, n_beads_list):
+        """Pack chains for fill_slots: (phys records, sim records, arena
+        doubles they need -- None when they need none)."""
+        n = len(phys_list)
+        same = n > 1 and all(p is phys_list[0] for p in phys_list) and all(s is sim_list[0] for s in sim_list) \
+            and all(k == n_beads_list[0] for k in n_beads_list)
+        if same:
+            # one ensemble: pack one record and replicate it
+            p1, s1, arena = _abi.pack_batch(phys_list[:1], sim_list[:1], n_beads_list[:1])
+            prec = (_abi.BdcuPhys * n)()
+            srec = (_abi.BdcuSim * n)()
+            ctypes.memmove(prec, ctypes.byref(p1[0]), ctypes.sizeof(_abi.BdcuPhys))
+            ctypes.memmove(srec, ctypes.byref(s1[0]), ctypes.sizeof(_abi.BdcuSim))
+            for dst, size in ((prec, ctypes.sizeof(_abi.BdcuPhys)), (srec, ctypes.sizeof(_abi.BdcuSim))):
+                filled = 1
+                while filled < n:  # doubling copies
+                    k = min(filled, n - filled)
+                    ctypes.memmove(ctypes.addressof(dst) + filled * size, ctypes.addressof(dst), k * size)
+                    filled += k
+        else:
+            prec, srec, arena = _abi.pack_batch(phys_list, sim_list, n_beads_list)
+        uses = any(prec[i].phi_offset >= 0 or prec[i].flow_n_times > 0 or prec[i].ext_n_entries > 0
+                   for i in range(min(n, 1) if same else n))
+        return prec, srec, (arena if uses else None)
+
+    def fill_slots(self, slots, phys_list, sim_list, n_beads_list, bead_offs, arena_base: int = 0,
+                   packed=None) -> int:
+        """Write the chains' tables into the context arena at arena_base and
+        fill the pool slots. Returns the number of arena doubles used."""
+        prec, srec, arena = packed if packed is not None else self.pack_slots(phys_list, sim_list, n_beads_list)
+        if arena is not None:
+            for i in range(len(slots)):
+                r = prec[i]
+                if r.phi_offset >= 0:
+                    r.phi_offset += arena_base
+                if r.flow_n_times > 0:
+                    r.flow_offset += arena_base
+                if r.ext_n_entries > 0:
+                    r.ext_offset += arena_base
+            self.write_arena(arena_base, arena)
+        self.update_chains(slots, prec, srec, bead_offs)
+        return 0 if arena is None else int(arena.size)
+
+    def write_arena(self, offset: int, values: np.ndarray):
+        self.use_stream()
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._ck(self.lib.bdcu_write_arena(self.h, int(offset), v.ctypes.data_as(_abi.c_double_p), v.size),
+                 "bdcu_write_arena")
+
+    def select(self, slots=None):
+        """The chains the next runs advance (None: every chain)."""
+        if slots is None:
+            self._ck(self.lib.bdcu_select(self.h, 0, None), "bdcu_select")
+            return
+        s = np.ascontiguousarray(slots, dtype=np.int32)
+        self._ck(self.lib.bdcu_select(self.h, len(s), s.ctypes.data_as(_abi.c_int32_p)), "bdcu_select")
+
     def ran1(self, rng_dev, n_per_chain: int, out_dev):
         self.use_stream()
         self._ck(self.lib.bdcu_ran1(self.h, int(rng_dev.shape[0]), dptr(rng_dev), int(n_per_chain),
@@ -156,6 +248,16 @@ class Ensemble:
         self._k.copy_(torch.as_tensor(np.broadcast_to(np.asarray(n_steps, dtype=np.int32), (self.n,)).copy()))
         self.ctx.run(self.R, self.rng, self.cache, self.cache_valid, self._t, self._k, self.status,
                      self.counters, self.form, cache_mode)
+
+    def plan(self) -> list:
+        """The launch plan of this ensemble's form: one dict per bucket."""
+        return self.ctx.describe_plan(self.form)
+
+    def autotune(self, probe_steps: int = 3) -> list:
+        """Choose the block-kernel launch shape per bucket by timing each on a
+        copy of the current state (the state itself is not advanced)."""
+        self._t.copy_(self.torch.as_tensor(np.array([s.time_start for s in self.sims], dtype=np.float64)))
+        return self.ctx.autotune(self.form, self.R, self.rng, self.cache, self.cache_valid, self._t, probe_steps)
 
     def reset_cache(self):
         self.cache_valid.zero_()

@@ -1,0 +1,396 @@
+"""Serving: continuous batching of ensemble jobs on one GPU.
+
+bdsim runs one ensemble per `simulate` call (python/bdsim/ensemble.py:238-277).
+A `Server` instead keeps a pool of chain slots resident on the device and
+admits jobs -- each the arguments of a `simulate` call -- while others run:
+
+  * admission: a job of n_traj chains of N beads needs n_traj consecutive
+    slots, n_traj*N consecutive beads of the pool (the pool is the HBM budget:
+    positions, warm-start vectors and the snapshot buffers) and room under the
+    active-chain cap; queued jobs are admitted in arrival order with a short
+    first-fit lookahead, and arrivals beyond the queue limit are rejected;
+  * each server iteration advances every running job by one chunk
+    (write_every steps, the job's snapshot interval) in ONE bdcu_run over all
+    their chains (buckets by bead count, device work lists), so jobs of
+    different N, n_traj and n_steps share the GPU;
+  * after each chunk the positions are copied on the device to a snapshot
+    buffer and from there to pinned host memory on a copy stream while the
+    next chunk runs; the host delivers each job's snapshot (and, at its last
+    step, its statuses) one iteration later and frees the slots of finished
+    jobs for the next admission;
+  * latency of a job = arrival to delivery of its last snapshot.
+
+A job's chains follow exactly the trajectory of `simulate` with the same
+arguments: trajectory i is seeded seed+i and starts from the same initial
+configuration, a chunk of k steps is one integrate span [t0, t0+(k-1)dt] with
+a cold spectral cache (CACHE_RESET_PER_CALL, the default), and the RNG stream
+carries across chunks.
+"""
+from __future__ import annotations
+
+import bisect
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._abi import CACHE_RESET_PER_CALL, COUNTER_FIELDS, ST_FATAL_MASK, count_steps
+from .engine import Context, _torch, form_code
+from .ensemble import INITIALIZERS, Initial, _segment, n_steps_of
+from .params import PhysParams, Rng, SimParams
+
+BYTES_PER_BEAD = 4 * 24  # R, warm-start cache, two snapshot buffers (FP64 xyz each)
+
+
+class Intervals:
+    """First-fit allocator of [0, capacity) in integer units."""
+
+    def __init__(self, capacity: int):
+        self.capacity = int(capacity)
+        self._free = [(0, self.capacity)]  # sorted, coalesced (start, length)
+
+    def alloc(self, n: int):
+        n = int(n)
+        for i, (s, L) in enumerate(self._free):
+            if L >= n:
+                if L == n:
+                    self._free.pop(i)
+                else:
+                    self._free[i] = (s + n, L - n)
+                return s
+        return None
+
+    def free(self, start: int, n: int):
+        if n <= 0:
+            return
+        i = bisect.bisect_left(self._free, (start, 0))
+        self._free.insert(i, (int(start), int(n)))
+        merged = []
+        for s, L in self._free:
+            if merged and merged[-1][0] + merged[-1][1] == s:
+                merged[-1] = (merged[-1][0], merged[-1][1] + L)
+            else:
+                merged.append((s, L))
+        self._free = merged
+
+    def used(self) -> int:
+        return self.capacity - sum(L for _, L in self._free)
+
+    def high_water(self) -> int:
+        """End of the last allocated unit (0 when empty)."""
+        if not self._free:
+            return self.capacity
+        s, L = self._free[-1]
+        return s if s + L == self.capacity else self.capacity
+
+
+@dataclass
+class Job:
+    """The arguments of one `simulate` call, plus its arrival time."""
+    phys: PhysParams
+    sim: SimParams
+    n_traj: int = 1
+    seed: int = 0
+    n_steps: int = None
+    initial: Initial = None
+    write_every: int = 0
+    keep_snapshots: bool = True
+    name: str = ""
+
+
+@dataclass
+class JobState:
+    job: Job
+    t_arrival: float
+    state: str = "queued"  # queued | running | done | rejected
+    t_admit: float = None
+    t_done: float = None
+    n_steps: int = 0
+    step: int = 0  # steps enqueued on the device
+    slot0: int = -1
+    bead0: int = -1
+    arena0: int = -1
+    arena_n: int = 0
+    n_beads: int = 0
+    steps: list = field(default_factory=list)
+    times: list = field(default_factory=list)
+    positions: list = field(default_factory=list)  # per snapshot: (n_traj, N, 3)
+    status: np.ndarray = None
+    counters: dict = None
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.t_arrival
+
+    def trajectories(self) -> np.ndarray:
+        """(n_traj, n_snap, N, 3) positions, the layout of `simulate`'s files."""
+        return np.stack(self.positions, axis=1)
+
+
+class Server:
+    """Continuous batching of ensemble jobs on one GPU (see the module text).
+
+    form: "mixed" or "plain"; max_chains: slots of the pool; bead_capacity:
+    beads of the pool (default: hbm_budget_bytes / BYTES_PER_BEAD);
+    max_active_chains: cap on running chains (None: the pool); queue_limit:
+    queued jobs beyond which arrivals are rejected (None: unbounded)."""
+
+    def __init__(self, device: int = 0, form="mixed", max_chains: int = 65536, bead_capacity: int = None,
+                 hbm_budget_bytes: int = 1 << 30, arena_capacity: int = 1 << 20, max_active_chains: int = None,
+                 queue_limit: int = None, lookahead: int = 16, cache_mode: int = CACHE_RESET_PER_CALL,
+                 on_snapshot=None, clock=time.monotonic):
+        torch = _torch()
+        self.torch = torch
+        self.form = form_code(form)
+        self.cache_mode = cache_mode
+        self.clock = clock
+        self.on_snapshot = on_snapshot
+        self.max_chains = int(max_chains)
+        self.bead_capacity = int(bead_capacity or max(1024, hbm_budget_bytes // BYTES_PER_BEAD))
+        self.max_active = int(max_active_chains or max_chains)
+        self.queue_limit = queue_limit
+        self.lookahead = int(lookahead)
+        dev = torch.device("cuda", device)
+        self.dev = dev
+        self.ctx = Context(device)
+        self.ctx.reserve(self.max_chains, self.bead_capacity, arena_capacity)
+        nb, nc = self.bead_capacity, self.max_chains
+        self.R = torch.zeros((nb, 3), dtype=torch.float64, device=dev)
+        self.cache = torch.zeros(3 * nb, dtype=torch.float64, device=dev)
+        self.rng = torch.zeros((nc, 3), dtype=torch.int32, device=dev)
+        self.valid = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self.counters = torch.zeros((nc, len(COUNTER_FIELDS)), dtype=torch.int64, device=dev)
+        self.t0 = torch.zeros(nc, dtype=torch.float64, device=dev)
+        self.k = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self.snap = [torch.zeros((nb, 3), dtype=torch.float64, device=dev) for _ in range(2)]
+        self.snap_host = [torch.empty((nb, 3), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+        self.status_host = [torch.empty(nc, dtype=torch.int32, pin_memory=True) for _ in range(2)]
+        self.tk_host = [(torch.zeros(nc, dtype=torch.float64, pin_memory=True),
+                         torch.zeros(nc, dtype=torch.int32, pin_memory=True)) for _ in range(2)]
+        self.tk_event = [None, None]
+        self.d2h_event = [None, None]
+        self.copy_stream = torch.cuda.Stream(device=dev)
+        self.slots = Intervals(nc)
+        self.beads = Intervals(nb)
+        self.arena = Intervals(arena_capacity)
+        self.queue: list[JobState] = []
+        self.running: list[JobState] = []
+        self.done: list[JobState] = []
+        self.rejected: list[JobState] = []
+        self._pending = None  # (parity, manifest) of the chunk whose snapshot is in flight
+        self._iter = 0
+        self._selected = None
+        self.active_chains = 0
+        self.chain_steps = 0
+        self.t_first = None
+
+    # ------------------------------------------------------------------ API
+
+    def submit(self, job: Job, arrival: float = None) -> JobState:
+        """Queue a job (arrival: a time of `clock`, default now)."""
+        js = JobState(job=job, t_arrival=self.clock() if arrival is None else arrival)
+        if self.t_first is None:
+            self.t_first = js.t_arrival
+        js.n_steps = int(job.n_steps) if job.n_steps is not None else n_steps_of(job.sim)
+        js.n_beads = int(job.phys.number_of_beads)
+        if self.queue_limit is not None and len(self.queue) >= self.queue_limit:
+            js.state = "rejected"
+            self.rejected.append(js)
+            return js
+        if job.n_traj > min(self.max_chains, self.max_active) or job.n_traj * js.n_beads > self.bead_capacity:
+            js.state = "rejected"
+            self.rejected.append(js)
+            return js
+        self.queue.append(js)
+        return js
+
+    def busy(self) -> bool:
+        return bool(self.queue or self.running or self._pending)
+
+    def step(self):
+        """One server iteration: admit, enqueue one chunk of every running job,
+        deliver the previous chunk's snapshots."""
+        self._admit()
+        launched = self._launch_chunk()
+        self._deliver()  # the chunk before: its copy ran while this one was queued
+        self._pending = launched
+
+    def run_until_idle(self, max_iters: int = 10 ** 9):
+        it = 0
+        while self.busy() and it < max_iters:
+            self.step()
+            it += 1
+
+    def run_stream(self, jobs, arrivals, horizon: float = None, drain: bool = True):
+        """Replay an arrival stream in real time: jobs[i] arrives arrivals[i]
+        seconds after the start. Stops admitting at `horizon` seconds (if
+        given) and, with drain, runs the admitted work to completion."""
+        order = np.argsort(arrivals, kind="stable")
+        t0 = self.clock()
+        i = 0
+        while True:
+            now = self.clock() - t0
+            while i < len(order) and arrivals[order[i]] <= now and (horizon is None or arrivals[order[i]] <= horizon):
+                self.submit(jobs[order[i]], arrival=t0 + arrivals[order[i]])
+                i += 1
+            more = i < len(order) and (horizon is None or arrivals[order[i]] <= horizon)
+            if not self.busy():
+                if not more:
+                    break
+                time.sleep(max(0.0, min(0.05, arrivals[order[i]] - now)))
+                continue
+            if horizon is not None and now > horizon and not drain:
+                break
+            self.step()
+        return self.stats(t0)
+
+    def stats(self, t0: float = None) -> dict:
+        lat = np.array([j.latency for j in self.done], dtype=np.float64)
+        svc = np.array([j.t_done - j.t_admit for j in self.done], dtype=np.float64)
+        t0 = self.t_first if t0 is None else t0
+        wall = (max(j.t_done for j in self.done) - t0) if self.done else 0.0
+        pct = (lambda a, q: float(np.percentile(a, q)) if a.size else None)
+        return {"jobs_completed": len(self.done), "jobs_rejected": len(self.rejected),
+                "jobs_queued": len(self.queue), "jobs_running": len(self.running),
+                "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+                "p50_service_s": pct(svc, 50), "p99_service_s": pct(svc, 99),
+                "chain_steps": int(self.chain_steps), "wall_s": wall,
+                "chain_steps_per_s": (self.chain_steps / wall) if wall > 0 else None}
+
+    # ------------------------------------------------------------ internals
+
+    def _admit(self):
+        torch = self.torch
+        i, looked = 0, 0
+        while i < len(self.queue) and looked < self.lookahead:
+            js = self.queue[i]
+            job = js.job
+            n, N = int(job.n_traj), js.n_beads
+            ok = self.active_chains + n <= self.max_active
+            s0 = self.slots.alloc(n) if ok else None
+            b0 = self.beads.alloc(n * N) if s0 is not None else None
+            if s0 is None or b0 is None:
+                if s0 is not None:
+                    self.slots.free(s0, n)
+                i += 1
+                looked += 1
+                continue
+            self.queue.pop(i)
+            init = job.initial or Initial()
+            R0s = [INITIALIZERS[init.method](N, job.seed + t, dict(init.kwargs)) for t in range(n)]
+            R0 = np.ascontiguousarray(np.concatenate(R0s).reshape(-1, 3), dtype=np.float64)
+            rng = np.array([Rng(job.seed + t).state() for t in range(n)], dtype=np.int32)
+            self.R[b0:b0 + n * N].copy_(torch.from_numpy(R0).pin_memory(), non_blocking=True)
+            self.rng[s0:s0 + n].copy_(torch.from_numpy(rng).pin_memory(), non_blocking=True)
+            self.valid[s0:s0 + n].zero_()
+            self.status[s0:s0 + n].zero_()
+            self.counters[s0:s0 + n].zero_()
+            packed = self.ctx.pack_slots([job.phys] * n, [job.sim] * n, [N] * n)
+            a0 = 0
+            if packed[2] is not None:
+                a0 = self.arena.alloc(packed[2].size)
+                if a0 is None:
+                    raise RuntimeError("serving arena exhausted (raise arena_capacity)")
+            used = self.ctx.fill_slots(list(range(s0, s0 + n)), None, None, None, [b0 + t * N for t in range(n)],
+                                       arena_base=a0, packed=packed)
+            js.slot0, js.bead0, js.arena0, js.arena_n = s0, b0, a0, used
+            js.state, js.t_admit = "running", self.clock()
+            js.steps.append(0)
+            js.times.append(float(job.sim.time_start))
+            if job.keep_snapshots:
+                js.positions.append(R0.reshape(n, N, 3).copy())
+            if self.on_snapshot is not None:
+                self.on_snapshot(js, 0, float(job.sim.time_start), R0.reshape(n, N, 3))
+            self.active_chains += n
+            self.running.append(js)
+
+    def _launch_chunk(self):
+        torch = self.torch
+        work = [js for js in self.running if js.step < js.n_steps]
+        if not work:
+            return None
+        par = self._iter & 1
+        self._iter += 1
+        if self.tk_event[par] is not None:
+            self.tk_event[par].synchronize()
+        th, kh = self.tk_host[par]
+        tn, kn = th.numpy(), kh.numpy()
+        manifest, sel = [], []
+        for js in work:
+            job, n = js.job, int(js.job.n_traj)
+            sim = job.sim
+            w = job.write_every if (job.write_every and job.write_every > 0) else js.n_steps
+            chunk = min(w, js.n_steps - js.step)
+            t0 = sim.time_start + js.step * sim.dt
+            k = count_steps(_segment(sim, t0, t0 + (chunk - 1) * sim.dt))
+            tn[js.slot0:js.slot0 + n] = t0
+            kn[js.slot0:js.slot0 + n] = k
+            sel.extend(range(js.slot0, js.slot0 + n))
+            js.step += chunk
+            self.chain_steps += n * k
+            manifest.append((js, js.step, sim.time_start + js.step * sim.dt, js.step >= js.n_steps))
+        hi_slot = max(js.slot0 + js.job.n_traj for js in work)
+        self.t0[:hi_slot].copy_(th[:hi_slot], non_blocking=True)
+        self.k[:hi_slot].copy_(kh[:hi_slot], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self.tk_event[par] = ev
+        key = tuple(sel)
+        if key != self._selected:
+            self.ctx.select(sel)
+            self._selected = key
+        self.ctx.run(self.R, self.rng, self.cache, self.valid, self.t0, self.k, self.status, self.counters,
+                     self.form, self.cache_mode)
+        hw = max(js.bead0 + js.job.n_traj * js.n_beads for js in work)
+        if self.d2h_event[par] is not None:
+            self.d2h_event[par].synchronize()  # the host buffer of two chunks ago is delivered
+        snap, host = self.snap[par], self.snap_host[par]
+        snap[:hw].copy_(self.R[:hw])
+        st_host = self.status_host[par]
+        done_copy = torch.cuda.Event()
+        done_copy.record()
+        with torch.cuda.stream(self.copy_stream):
+            self.copy_stream.wait_event(done_copy)
+            host[:hw].copy_(snap[:hw], non_blocking=True)
+            st_host[:hi_slot].copy_(self.status[:hi_slot], non_blocking=True)
+            ev2 = torch.cuda.Event()
+            ev2.record(self.copy_stream)
+        self.d2h_event[par] = ev2
+        return (par, manifest)
+
+    def _deliver(self):
+        if self._pending is None:
+            return
+        par, manifest = self._pending
+        self._pending = None
+        self.d2h_event[par].synchronize()
+        host = self.snap_host[par].numpy()
+        sth = self.status_host[par].numpy()
+        now = self.clock()
+        for js, step, t, final in manifest:
+            n, N = int(js.job.n_traj), js.n_beads
+            rows = host[js.bead0:js.bead0 + n * N].reshape(n, N, 3)
+            js.steps.append(step)
+            js.times.append(t)
+            if js.job.keep_snapshots:
+                js.positions.append(rows.copy())
+            if self.on_snapshot is not None:
+                self.on_snapshot(js, step, t, rows)
+            if final:
+                js.status = sth[js.slot0:js.slot0 + n].copy()
+                js.state, js.t_done = "done", now
+                self._retire(js)
+
+    def _retire(self, js: JobState):
+        n = int(js.job.n_traj)
+        self.running.remove(js)
+        self.done.append(js)
+        self.slots.free(js.slot0, n)
+        self.beads.free(js.bead0, n * js.n_beads)
+        if js.arena_n:
+            self.arena.free(js.arena0, js.arena_n)
+        self.active_chains -= n
+
+    def failed(self, js: JobState) -> np.ndarray:
+        return (js.status & ST_FATAL_MASK) != 0

@@ -200,6 +200,33 @@ def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
     return n * CHUNK * steps / wall, h2d, d2h
 
 
+def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed", queue_limit=256,
+                max_active=16384, drain=False):
+    """The serving workload: Poisson job arrivals replayed in real time
+    against the continuous-batching server for `horizon` seconds. Jobs: N ~
+    U{10..300}, n_traj ~ U{1..256}, n_steps log-uniform [1e3, 1e5] (times
+    scale_steps), shear or uniaxial at U[0.1, 5], FENE b=100, h*=0.25
+    Chebyshev, write_every=100. Snapshots are copied to pinned host memory
+    and delivered every chunk (not kept)."""
+    from bdsim_b200 import serving, workloads
+    specs = workloads.serving_jobs(rate=rate, duration=horizon, seed=seed)
+    jobs, arrivals = [], []
+    for sp in specs:
+        ns = max(100, int(round(sp.n_steps * scale_steps)))
+        jobs.append(serving.Job(phys=sp.phys, sim=sp.sim, n_traj=sp.n_traj, seed=sp.seed, n_steps=ns,
+                                write_every=sp.write_every, keep_snapshots=False))
+        arrivals.append(sp.arrival)
+    srv = serving.Server(device=torch.cuda.current_device(), form=form, max_chains=max_active,
+                         hbm_budget_bytes=2 << 30, queue_limit=queue_limit, max_active_chains=max_active)
+    torch.cuda.synchronize()
+    st = srv.run_stream(jobs, np.asarray(arrivals), horizon=horizon, drain=drain)
+    torch.cuda.synchronize()
+    st.update({"jobs_offered": len(jobs), "horizon_s": horizon, "rate_jobs_per_s": rate,
+               "n_steps_scale": scale_steps, "queue_limit": queue_limit, "max_active_chains": max_active,
+               "offered_chain_steps": int(sum(j.n_traj * j.n_steps for j in jobs))})
+    return st
+
+
 def cpu_reference(seconds_target=15.0, threads=None):
     """The reference C++ step (oracle/_ref, compiled from the reference
     sources; the C restatement when that library is absent) on the host

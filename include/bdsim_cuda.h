@@ -197,6 +197,8 @@ int bdcu_count_steps(const bdcu_sim* sim, int64_t* n_steps_out);
      n_steps      n_chains int32, steps to take in this call
      status       n_chains int32, OR-ed with BDCU_ST_* bits
      counters     n_chains bdcu_counters, accumulated
+   (for a slot pool: bead_capacity and n_slots in place of total_beads and
+   n_chains). Only the selected chains (bdcu_select; default all) are touched.
    A chain whose status has a fatal bit set is skipped. */
 int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache,
              int32_t* cache_valid, const double* t_start, const int32_t* n_steps,
@@ -225,14 +227,79 @@ int bdcu_forces(bdcu_ctx* ctx, const double* R, double t, int which, double* F);
    int32, advanced in place) into out (device, n_chains*n_per_chain). */
 int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double* out);
 
+/* ---- Launch plans for batches of uneven chains (no counterpart in the
+   reference, which integrates one chain per call: time_integrate_chain,
+   src/integrator.hpp:32).
+   bdcu_run splits the chains it advances into buckets by bead count and runs
+   each bucket as one persistent launch over a device work list ordered
+   largest chain first; buckets run concurrently, forked from the context
+   stream and joined back to it. In the FP32-mixed form a chain of N <= 512
+   beads (and no Cholesky method) runs on a team of 1, 2, 4 or 8 warps (N <=
+   64, 128, 256, 512; buckets 0..3); every other chain runs one chain per
+   thread block, in buckets 4..7 split at N = 64, 128 and 256. Once a plan is
+   built (first bdcu_run after a change of records, selection or form) a
+   bdcu_run enqueues only a memset, event records/waits and kernel launches,
+   so it may be captured in a CUDA graph. */
+enum { BDCU_KERNEL_BLOCK = 0, BDCU_KERNEL_TEAM = 1 };
+#define BDCU_MAX_BUCKETS 8
+typedef struct bdcu_bucket_info {
+    int32_t bucket;      /* 0..3: team kernel; 4..7: block kernel */
+    int32_t kernel;      /* BDCU_KERNEL_* */
+    int32_t team_warps;  /* team kernel: warps per chain (0 for the block kernel) */
+    int32_t n_chains;    /* chains in the bucket */
+    int32_t min_beads;
+    int32_t max_beads;
+    int32_t block;       /* threads per block */
+    int32_t grid;        /* persistent blocks */
+    int32_t v_cap;       /* Lanczos basis vectors kept in shared memory */
+    int32_t d_in_smem;   /* dense D in shared memory (plain form) */
+    int32_t tuned;       /* 1: shape chosen by bdcu_autotune */
+    int32_t reserved;
+    int64_t smem_bytes;  /* dynamic shared memory per block */
+} bdcu_bucket_info;
+/* The plan bdcu_run would use for `form` on the current selection; writes up
+   to `cap` buckets (cap >= BDCU_MAX_BUCKETS always suffices) and their count. */
+int bdcu_describe_plan(bdcu_ctx* ctx, int form, bdcu_bucket_info* out, int cap, int* n_out);
+
+/* Time every launch shape of each block-kernel bucket of the current selection
+   (threads per block x Lanczos vectors in shared memory x, in the plain form,
+   D in shared memory) for probe_steps steps on device copies of the given state
+   -- the caller's buffers are read, never written -- and keep the fastest shape
+   per (form, bucket) for later bdcu_run calls. Synchronous; allocates and frees
+   its copies. The shape changes only the speed and, through block reductions,
+   the rounding of the Lanczos and Chebyshev dot products. */
+int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, const double* cache,
+                  const int32_t* cache_valid, const double* t_start, int probe_steps);
+
+/* ---- Slot pools, for a serving loop that admits and retires chains between
+   runs (no counterpart in the reference).
+   bdcu_reserve replaces the context's chains with n_slots empty slots, sized
+   for state arrays of bead_capacity beads (R and cache hold bead_capacity*3
+   doubles; rng n_slots*3 int32; cache_valid, t_start, n_steps, status n_slots;
+   counters n_slots records) and an arena of arena_len doubles (zeroed). */
+int bdcu_reserve(bdcu_ctx* ctx, int n_slots, int64_t bead_capacity, int64_t arena_len);
+/* Fill `count` slots with chains: slot ids (host), their phys/sim records and
+   the first bead of each chain in the state arrays (bead_off + n_beads <=
+   bead_capacity). Table offsets in phys refer to the context arena. Enqueued on
+   the context stream; the records are derived on the host. */
+int bdcu_update_chains(bdcu_ctx* ctx, int count, const int32_t* slots, const bdcu_phys* phys,
+                       const bdcu_sim* sim, const int64_t* bead_off);
+/* Copy `count` doubles (host) into the context arena at `offset`. */
+int bdcu_write_arena(bdcu_ctx* ctx, int64_t offset, const double* values, int64_t count);
+/* The chains the following bdcu_run calls advance: `count` slot ids (host),
+   distinct, filled, with disjoint bead ranges; count = 0 with slots = NULL
+   selects every chain (not allowed for a pool). */
+int bdcu_select(bdcu_ctx* ctx, int count, const int32_t* slots);
+
 /* bdcu_run for callers that cannot allocate device memory. No counterpart in
    the reference: bdsim runs on the CPU and never allocates GPU memory.
    Some callers cannot call cudaMalloc -- a host application whose memory pool
    already owns the GPU's memory, or a serving loop that must not take the
    implicit device-wide synchronisation cudaMalloc/cudaFree imply. This entry
    point takes the parameters on the host (as bdcu_set_chains does) and runs
-   the same integrator kernel as bdcu_run on the caller's device buffers; the
-   parameter records, arena, work counter and per-block scratch live in one
+   the same kernels as bdcu_run (its buckets, one after another) on the
+   caller's device buffers; the parameter records, work lists, arena, work
+   counters and per-block scratch live in one
    file-scope device array of BDCU_STATIC_SCRATCH_BYTES that every GPU using
    the library holds until process exit. It calls no cudaMalloc/cudaFree.
    ctx comes from bdcu_create (which allocates no device memory) and supplies
@@ -243,7 +310,7 @@ int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double
    - The first call on a device takes the array's device address
      (cudaGetSymbolAddress): make it before any stream capture on that device.
    - Every call shares the array and leaves its contents behind; the work
-     counter is cleared by each call. Calls that overlap on the GPU race on the
+     counters are cleared by each call. Calls that overlap on the GPU race on the
      array: serialise them. */
 #define BDCU_STATIC_SCRATCH_BYTES (16u * 1024u * 1024u)
 int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bdcu_sim* sim,

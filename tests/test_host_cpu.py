@@ -62,7 +62,8 @@ def test_abi_struct_layout_matches_header(tmp_path):
     if cc is None:
         pytest.skip("no C compiler")
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bdsim_cuda.h"', "int main(void) {"]
-    for cname, cls in (("bdcu_phys", _abi.BdcuPhys), ("bdcu_sim", _abi.BdcuSim), ("bdcu_counters", _abi.BdcuCounters)):
+    for cname, cls in (("bdcu_phys", _abi.BdcuPhys), ("bdcu_sim", _abi.BdcuSim), ("bdcu_counters", _abi.BdcuCounters),
+                       ("bdcu_bucket_info", _abi.BdcuBucketInfo)):
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for fname, _ in cls._fields_:
             lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
@@ -73,7 +74,8 @@ def test_abi_struct_layout_matches_header(tmp_path):
     subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
     c_layout = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
-    for cname, cls in (("bdcu_phys", _abi.BdcuPhys), ("bdcu_sim", _abi.BdcuSim), ("bdcu_counters", _abi.BdcuCounters)):
+    for cname, cls in (("bdcu_phys", _abi.BdcuPhys), ("bdcu_sim", _abi.BdcuSim), ("bdcu_counters", _abi.BdcuCounters),
+                       ("bdcu_bucket_info", _abi.BdcuBucketInfo)):
         assert c_layout[(cname, "size")] == ctypes.sizeof(cls)
         for fname, _ in cls._fields_:
             assert c_layout[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
