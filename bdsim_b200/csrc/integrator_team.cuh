@@ -97,6 +97,99 @@ static __device__ void halfwarp_bisect(const double* al, const double* bb, int k
     }
 }
 
+// Sturm count below x for a tridiagonal of k <= kLanczosWarm entries held in
+// registers (a: diagonal, b: off-diagonal), the divide-free recurrence of
+// sturm_count_products fully unrolled.
+__device__ __forceinline__ int sturm_count_reg(const double (&a)[kLanczosWarm], const double (&b)[kLanczosWarm], int k,
+                                               double x) {
+    double pm = 1.0, p = a[0] - x;
+    int count = (p < 0.0) ? 1 : 0;
+#pragma unroll
+    for (int i = 1; i < kLanczosWarm; ++i) {
+        if (i < k) {
+            const double pn = (a[i] - x) * p - (b[i - 1] * b[i - 1]) * pm;
+            count += ((pn < 0.0) != (p < 0.0)) ? 1 : 0;
+            pm = p;
+            p = pn;
+            if (fabs(p) > 1e150) {
+                p *= 1e-150;
+                pm *= 1e-150;
+            }
+        }
+    }
+    return count;
+}
+
+// Multisection for the target-th eigenvalue boundary on a half warp: 15 lanes
+// evaluate the Sturm count at 15 evenly spaced interior points of [lo, hi], a
+// ballot finds the sixteenth that holds the boundary (4 bits per round), the
+// iteration of src/hydrodynamics.cpp:251-260 in place of its halvings. Every
+// lane of the half warp ends with the same lo, hi.
+static __device__ void halfwarp_multisect(const double (&a)[kLanczosWarm], const double (&b)[kLanczosWarm], int k,
+                                          int target, double& lo, double& hi) {
+    const int h = threadIdx.x & 15;
+    const int shift = threadIdx.x & 16;
+    for (int it = 0; it < 25; ++it) {
+        const double w = hi - lo;
+        const bool ge = h < 15 && sturm_count_reg(a, b, k, lo + w * ((double)(h + 1) * 0.0625)) >= target;
+        const unsigned bal = (__ballot_sync(kFull, ge) >> shift) & 0xffffu;
+        const int f = bal ? __ffs(bal) - 1 : 15;
+        const double nlo = f == 0 ? lo : lo + w * ((double)f * 0.0625);
+        const double nhi = f == 15 ? hi : lo + w * ((double)(f + 1) * 0.0625);
+        // settled: the interval stopped shrinking or is within 1e-10 relative
+        // (the bounds are padded by 2x / 2% downstream)
+        const bool done = (nlo == lo && nhi == hi) || (nhi - nlo) <= 1e-10 * fmax(fabs(nlo), fabs(nhi));
+        lo = nlo;
+        hi = nhi;
+        if (__all_sync(kFull, done)) break;
+    }
+}
+
+// Inverse iteration for a Ritz vector (src/hydrodynamics.cpp:106-136) with the
+// tridiagonal (k <= kLanczosWarm) in registers; every lane that calls it
+// computes the same y.
+static __device__ void tridiag_vec_reg(const double (&a)[kLanczosWarm], const double (&b)[kLanczosWarm], int m,
+                                       double lambda, double (&y)[kLanczosWarm]) {
+    const double scale = dmax_(fabs(lambda), 1.0);
+    const double shift = lambda - 1.0e-7 * scale;
+    const double y0 = rsqrt((double)m);
+    double c[kLanczosWarm];
+#pragma unroll
+    for (int i = 0; i < kLanczosWarm; ++i) y[i] = i < m ? y0 : 0.0;
+    for (int it = 0; it < 2; ++it) {
+        double beta = a[0] - shift;
+        if (fabs(beta) < 1.0e-300) beta = 1.0e-300;
+        double ib = 1.0 / beta;
+        c[0] = (m > 1 ? b[0] * ib : 0.0);
+        y[0] = y[0] * ib;
+#pragma unroll
+        for (int i = 1; i < kLanczosWarm; ++i) {
+            if (i < m) {
+                beta = (a[i] - shift) - b[i - 1] * c[i - 1];
+                if (fabs(beta) < 1.0e-300) beta = 1.0e-300;
+                ib = 1.0 / beta;
+                c[i] = (i < m - 1 ? b[i] * ib : 0.0);
+                y[i] = (y[i] - b[i - 1] * y[i - 1]) * ib;
+            }
+        }
+#pragma unroll
+        for (int i = kLanczosWarm - 2; i >= 0; --i)
+            if (i < m - 1) y[i] = y[i] - c[i] * y[i + 1];
+        double nrm = 0.0;
+#pragma unroll
+        for (int i = 0; i < kLanczosWarm; ++i) nrm += y[i] * y[i];
+        nrm = sqrt(nrm);
+        if (!(nrm > 0.0) || !isfinite(nrm)) {
+#pragma unroll
+            for (int i = 0; i < kLanczosWarm; ++i) y[i] = i < m ? y0 : 0.0;
+            return;
+        }
+        const double inr = 1.0 / nrm;
+#pragma unroll
+        for (int i = 0; i < kLanczosWarm; ++i) y[i] *= inr;
+    }
+}
+
 // Inverse iteration for a Ritz vector (src/hydrodynamics.cpp:106-136), one lane.
 static __device__ void wk_tridiag_vec(const double* a, const double* b, int m, double lambda, double* y, double* c,
                                       double* d) {
@@ -149,7 +242,7 @@ struct TeamChain {
     int team;       // team in the thread block (named barrier 1 + team)
     int N, n;
     bool hi;
-    int64_t cnt[8];
+    int32_t cnt[8];  // this call's counts for the chain (added to the 64-bit counters at the end)
     int status;
     // RPY constants (FP32). Bead coordinates are staged divided by `scale`
     // (= h* under HI), which turns the RPY weights into functions of
@@ -179,24 +272,47 @@ struct TeamChain {
         }
     }
 
-    // Eight team sums at once (the batched projections of the warm Lanczos).
+    // Eight team sums at once (the batched projections of the warm Lanczos),
+    // the same bits in every thread. In each warp a transposed reduction:
+    // exchange halves of the vector with lane^16, ^8, ^4 (each lane keeps the
+    // half its lane bit selects), then a butterfly over lane^2, ^1, leaves sum
+    // u = 4*b4 + 2*b3 + b2 in the lanes whose bits 4, 3, 2 are b4, b3, b2;
+    // lanes 0, 4, ..., 28 publish the warp's eight sums in shared memory and
+    // the warps' partials are added in warp order.
     __device__ void tsum8(double (&c)[kLanczosWarm]) const {
+        static_assert(kLanczosWarm == 8, "tsum8 reduces eight values");
+        const bool u16 = wl & 16, u8 = wl & 8, u4 = wl & 4;
+        double k4[4], k2[2];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+        for (int u = 0; u < 4; ++u) {
+            const double send = u16 ? c[u] : c[u + 4];
+            k4[u] = (u16 ? c[u + 4] : c[u]) + __shfl_xor_sync(kFull, send, 16);
+        }
 #pragma unroll
-            for (int u = 0; u < kLanczosWarm; ++u) c[u] += __shfl_xor_sync(kFull, c[u], o);
-        if constexpr (T > 1) {
+        for (int u = 0; u < 2; ++u) {
+            const double send = u8 ? k4[u] : k4[u + 2];
+            k2[u] = (u8 ? k4[u + 2] : k4[u]) + __shfl_xor_sync(kFull, send, 8);
+        }
+        double s = (u4 ? k2[1] : k2[0]) + __shfl_xor_sync(kFull, u4 ? k2[0] : k2[1], 4);
+        s += __shfl_xor_sync(kFull, s, 2);
+        s += __shfl_xor_sync(kFull, s, 1);
+        const int idx = (u16 ? 4 : 0) + (u8 ? 2 : 0) + (u4 ? 1 : 0);
+        if constexpr (T == 1) {
+            if ((wl & 3) == 0) S.red[idx] = s;
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < kLanczosWarm; ++u) c[u] = S.red[u];
+            __syncwarp();
+        } else {
             sync();
-            if (wl == 0)
-#pragma unroll
-                for (int u = 0; u < kLanczosWarm; ++u) S.red[kLanczosWarm * wi + u] = c[u];
+            if ((wl & 3) == 0) S.red[kLanczosWarm * wi + idx] = s;
             sync();
 #pragma unroll
             for (int u = 0; u < kLanczosWarm; ++u) {
-                double s = S.red[u];
+                double v = S.red[u];
 #pragma unroll
-                for (int w = 1; w < T; ++w) s += S.red[kLanczosWarm * w + u];
-                c[u] = s;
+                for (int w = 1; w < T; ++w) v += S.red[kLanczosWarm * w + u];
+                c[u] = v;
             }
         }
     }
@@ -577,13 +693,15 @@ struct TeamChain {
         int k = 0;
         double b = 0.0;
         if (m <= kLanczosWarm) {
-            // warm runs: classical Gram-Schmidt applied twice against the whole
-            // basis, each pass's projections reduced together; the projection
-            // on v_j is alpha_j
+            // warm runs: classical Gram-Schmidt against the whole basis, each
+            // pass's projections reduced together; the projection on v_j is
+            // alpha_j. A second pass runs when the first removed more than
+            // half of |w|^2 (the DGKS criterion |w'|^2 < sum c_u^2: w lost
+            // over 1/sqrt(2) of its norm to the projections).
             for (int j = 0; j < m; ++j) {
                 store(basis(j, m), v);
                 apply(v, w);
-                double al = 0.0;
+                double al = 0.0, bsq = 0.0;
                 for (int pass = 0; pass < 2; ++pass) {
                     double c[kLanczosWarm];
 #pragma unroll
@@ -610,13 +728,18 @@ struct TeamChain {
                                     if (valid(q)) w[q][d] -= c[u] * vu[3 * bead(q) + d];
                         }
                     }
+                    double p2 = 0.0;
 #pragma unroll
-                    for (int u = 0; u < kLanczosWarm; ++u)
+                    for (int u = 0; u < kLanczosWarm; ++u) {
                         if (u == j) al += c[u];
+                        if (u <= j) p2 += c[u] * c[u];
+                    }
+                    bsq = dot(w, w);
+                    if (pass == 0 && bsq >= p2) break;
                 }
                 if (tid == 0) S.alpha[k] = al;
                 ++k;
-                b = sqrt(dot(w, w));
+                b = sqrt(bsq);
                 if (b < 1.0e-10) break;
                 const double ib = 1.0 / b;
 #pragma unroll
@@ -667,7 +790,37 @@ struct TeamChain {
             load(basis(0, m), vmax);
             return 1;
         }
-        if (wi == 0) {
+        if (wi == 0 && k <= kLanczosWarm) {
+            // warm-sized tridiagonal in registers: Gershgorin bracket, then
+            // lanes 0-15 find the smallest eigenvalue and its Ritz vector,
+            // lanes 16-31 the largest
+            double ar[kLanczosWarm], br[kLanczosWarm];
+#pragma unroll
+            for (int i = 0; i < kLanczosWarm; ++i) {
+                ar[i] = i < k ? S.alpha[i] : 0.0;
+                br[i] = i < k - 1 ? S.beta[i] : 0.0;
+            }
+            double lo = ar[0], hi2 = ar[0];
+#pragma unroll
+            for (int i = 0; i < kLanczosWarm; ++i) {
+                if (i < k) {
+                    const double rad = (i > 0 ? fabs(br[i - 1]) : 0.0) + fabs(br[i]);
+                    lo = dmin_(lo, ar[i] - rad);
+                    hi2 = dmax_(hi2, ar[i] + rad);
+                }
+            }
+            halfwarp_multisect(ar, br, k, wl < 16 ? 1 : k, lo, hi2);
+            const double r = 0.5 * (lo + hi2);
+            double y[kLanczosWarm];
+            tridiag_vec_reg(ar, br, k, r, y);
+            if ((wl & 15) == 0) {
+                double* dst = wl == 0 ? S.ymin : S.ymax;
+#pragma unroll
+                for (int i = 0; i < kLanczosWarm; ++i)
+                    if (i < k) dst[i] = y[i];
+                S.rr[wl >> 4] = r;
+            }
+        } else if (wi == 0) {
             double lo = S.alpha[0], hi2 = S.alpha[0];
             for (int i = 0; i < k; ++i) {
                 const double rad = (i > 0 ? fabs(S.beta[i - 1]) : 0.0) + (i < k - 1 ? fabs(S.beta[i]) : 0.0);
@@ -1030,22 +1183,19 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             W.stage_pos(Rp);
             float Fep[2][3], dummy[2][3];
             W.forces(Rp, t + dt, dummy, Fep, false);
+            // D Fs + D (Fe + Fe~) = D (Fs + Fe) + D Fe~: the predictor's
+            // product plus one more (the reference forms both sums anew)
             W.stage_pos(R);
-            float DFs[2][3], DFe[2][3];
+            float DFep[2][3];
             double ups[2][3];
-            W.applyF(Fs, DFs);
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) A[q][d] = Fe[q][d] + Fep[q][d];
-            W.applyF(A, DFe);
+            W.applyF(Fep, DFep);
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
                     const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
                     const double fl2 = K2[3 * r] * Rp[q][0] + K2[3 * r + 1] * Rp[q][1] + K2[3 * r + 2] * Rp[q][2];
-                    ups[q][r] = R[q][r] + dt * (0.5 * (fl1 + fl2) + 0.125 * DFs[q][r] + 0.125 * DFe[q][r]) +
+                    ups[q][r] = R[q][r] + dt * (0.5 * (fl1 + fl2) + 0.125 * ((double)DF[q][r] + (double)DFep[q][r])) +
                                 sqrt2inv * dW[q][r];
                 }
             // solve_connectors (src/integrator.cpp:125-165): thread owns bonds bead(0), bead(1)
@@ -1227,7 +1377,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             a.cache_valid[c] = cache_valid;
             a.status[c] = W.status;
             int64_t* cc = reinterpret_cast<int64_t*>(a.counters + c);
-            for (int k = 0; k < 8; ++k) cc[k] += W.cnt[k];
+            for (int k = 0; k < 8; ++k) cc[k] += (int64_t)W.cnt[k];
         }
         team_sync<T>(team);
     }
