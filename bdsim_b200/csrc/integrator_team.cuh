@@ -136,13 +136,24 @@ static __device__ void halfwarp_multisect(const double (&a)[kLanczosWarm], const
         const int f = bal ? __ffs(bal) - 1 : 15;
         const double nlo = f == 0 ? lo : lo + w * ((double)f * 0.0625);
         const double nhi = f == 15 ? hi : lo + w * ((double)(f + 1) * 0.0625);
-        // settled: the interval stopped shrinking or is within 1e-10 relative
-        // (the bounds are padded by 2x / 2% downstream)
-        const bool done = (nlo == lo && nhi == hi) || (nhi - nlo) <= 1e-10 * fmax(fabs(nlo), fabs(nhi));
+        // settled: the interval stopped shrinking or is within 1e-6 relative
+        // (the bounds are padded by 2x / 2% downstream, and the FD check
+        // polices the Chebyshev result)
+        const bool done = (nlo == lo && nhi == hi) || (nhi - nlo) <= 1e-6 * fmax(fabs(nlo), fabs(nhi));
         lo = nlo;
         hi = nhi;
         if (__all_sync(kFull, done)) break;
     }
+}
+
+// 1/x for |x| in [1e-30, 1e30]: a single-precision seed refined by two
+// Newton-Raphson steps r <- r (2 - x r) (quadratic convergence: 2^-23 ->
+// 2^-46 -> below double rounding).
+__device__ __forceinline__ double rcp_newton(double x) {
+    double r = (double)__frcp_rn((float)x);
+    r = r * (2.0 - x * r);
+    r = r * (2.0 - x * r);
+    return r;
 }
 
 // Inverse iteration for a Ritz vector (src/hydrodynamics.cpp:106-136) with the
@@ -157,17 +168,20 @@ static __device__ void tridiag_vec_reg(const double (&a)[kLanczosWarm], const do
 #pragma unroll
     for (int i = 0; i < kLanczosWarm; ++i) y[i] = i < m ? y0 : 0.0;
     for (int it = 0; it < 2; ++it) {
+        // pivots: the reference's tiny-pivot guard (1e-300) raised to 1e-30 so
+        // that the reciprocal's single-precision seed stays in range (the
+        // vector only seeds the next step's Lanczos)
         double beta = a[0] - shift;
-        if (fabs(beta) < 1.0e-300) beta = 1.0e-300;
-        double ib = 1.0 / beta;
+        if (fabs(beta) < 1.0e-30) beta = 1.0e-30;
+        double ib = rcp_newton(beta);
         c[0] = (m > 1 ? b[0] * ib : 0.0);
         y[0] = y[0] * ib;
 #pragma unroll
         for (int i = 1; i < kLanczosWarm; ++i) {
             if (i < m) {
                 beta = (a[i] - shift) - b[i - 1] * c[i - 1];
-                if (fabs(beta) < 1.0e-300) beta = 1.0e-300;
-                ib = 1.0 / beta;
+                if (fabs(beta) < 1.0e-30) beta = 1.0e-30;
+                ib = rcp_newton(beta);
                 c[i] = (i < m - 1 ? b[i] * ib : 0.0);
                 y[i] = (y[i] - b[i - 1] * y[i - 1]) * ib;
             }
@@ -335,18 +349,33 @@ struct TeamChain {
 
     // ---- FP32 matrix-free D.x (Diffusion::apply, src/mobility.cpp:53-56;
     // RPY weights src/hydrodynamics.cpp:77-105). x, y: the thread's two beads.
-    __device__ void apply32(const float (&x)[2][3], float (&acc)[2][3]) {
-        cnt[C_DX] += 1;
+    // K products against the same D in one pass over the bead pairs: the
+    // pair geometry and weights are computed once for all K inputs (K = 3
+    // for the products of a step that do not depend on one another).
+    // Inputs are staged in S.xs and, for K > 1, in S.s1 / S.s2 viewed as
+    // float4 (free while the mobility products run).
+    template <int K>
+    __device__ void applyK(const float (&x)[K][2][3], float (&acc)[K][2][3]) {
+        static_assert(K >= 1 && K <= 3, "applyK stages at most three inputs");
+        static_assert(offsetof(TeamShared<T>, s1) % 16 == 0 && offsetof(TeamShared<T>, s2) % 16 == 0 &&
+                          sizeof(TeamShared<T>::s1) >= sizeof(float4) * 64 * T,
+                      "s1 / s2 must hold a 16-byte aligned float4 per bead");
+        cnt[C_DX] += K;
+        float4* stage[3] = {S.xs, reinterpret_cast<float4*>(S.s1), reinterpret_cast<float4*>(S.s2)};
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-            if (valid(q)) S.xs[bead(q)] = make_float4(x[q][0], x[q][1], x[q][2], 0.f);
+            if (valid(q))
+#pragma unroll
+                for (int r = 0; r < K; ++r) stage[r][bead(q)] = make_float4(x[r][q][0], x[r][q][1], x[r][q][2], 0.f);
         sync();
         float4 pb[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             pb[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) acc[q][d] = 0.f;
+            for (int r = 0; r < K; ++r)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
         }
         // In units of h*: with d = (R_j - R_b)/h*, s = |d|^2, rho = s^-1/2,
         //   far  (s >= 4 pi): om1 = rho (K1 + K2 rho^2), om2 = rho^3 (K1 - K3 rho^2)
@@ -356,32 +385,16 @@ struct TeamChain {
         // om2 d = 0: it contributes the identity block.
         bool one_slot = false;
         if constexpr (T > 1) one_slot = __all_sync(kFull, !valid(1));
-        if (one_slot) {
-            // the second bead slot is empty in every lane of this warp: only
-            // slot 0 does work (half the pairs)
+        const int nq = one_slot ? 1 : 2;
 #pragma unroll 2
-            for (int j = 0; j < N; ++j) {
-                const float4 pj = S.pos[j];
-                const float4 xj = S.xs[j];
-                const float dx = pj.x - pb[0].x, dy = pj.y - pb[0].y, dz = pj.z - pb[0].z;
-                const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
-                const float rho = rsqrtf(sq);
-                const float rho2 = rho * rho;
-                const bool far = sq >= 12.566370614359172f;
-                const float om1 = far ? rho * (K1 + K2 * rho2) : 1.f - C3 * (sq * rho);
-                const float om2 = far ? (rho * rho2) * (K1 - K3 * rho2) : C7 * rho;
-                const float tt = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
-                acc[0][0] += om1 * xj.x + tt * dx;
-                acc[0][1] += om1 * xj.y + tt * dy;
-                acc[0][2] += om1 * xj.z + tt * dz;
-            }
-        } else {
-#pragma unroll 2
-            for (int j = 0; j < N; ++j) {
-                const float4 pj = S.pos[j];
-                const float4 xj = S.xs[j];
+        for (int j = 0; j < N; ++j) {
+            const float4 pj = S.pos[j];
+            float4 xj[K];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
+            for (int r = 0; r < K; ++r) xj[r] = stage[r][j];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (q < nq) {
                     const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
                     const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
                     const float rho = rsqrtf(sq);
@@ -389,10 +402,13 @@ struct TeamChain {
                     const bool far = sq >= 12.566370614359172f;
                     const float om1 = far ? rho * (K1 + K2 * rho2) : 1.f - C3 * (sq * rho);
                     const float om2 = far ? (rho * rho2) * (K1 - K3 * rho2) : C7 * rho;
-                    const float tt = om2 * (dx * xj.x + dy * xj.y + dz * xj.z);
-                    acc[q][0] += om1 * xj.x + tt * dx;
-                    acc[q][1] += om1 * xj.y + tt * dy;
-                    acc[q][2] += om1 * xj.z + tt * dz;
+#pragma unroll
+                    for (int r = 0; r < K; ++r) {
+                        const float tt = om2 * (dx * xj[r].x + dy * xj[r].y + dz * xj[r].z);
+                        acc[r][q][0] += om1 * xj[r].x + tt * dx;
+                        acc[r][q][1] += om1 * xj[r].y + tt * dy;
+                        acc[r][q][2] += om1 * xj[r].z + tt * dz;
+                    }
                 }
             }
         }
@@ -401,7 +417,13 @@ struct TeamChain {
         for (int q = 0; q < 2; ++q)
             if (!valid(q))
 #pragma unroll
-                for (int d = 0; d < 3; ++d) acc[q][d] = 0.f;
+                for (int r = 0; r < K; ++r)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
+    }
+
+    __device__ void apply32(const float (&x)[2][3], float (&acc)[2][3]) {
+        applyK<1>(reinterpret_cast<const float(&)[1][2][3]>(x), reinterpret_cast<float(&)[1][2][3]>(acc));
     }
 
     __device__ void apply(const double (&x)[2][3], double (&y)[2][3]) {
@@ -661,31 +683,37 @@ struct TeamChain {
                 for (int d = 0; d < 3; ++d) vec[3 * bead(q) + d] = x[q][d];
     }
 
-    // Returns the number of Lanczos steps; sets rmin/rmax and the Ritz vectors.
-    __device__ int lanczos(int m, bool warm, const double* cache, double (&vmin)[2][3], double (&vmax)[2][3],
-                           double& rmin, double& rmax) {
-        if (n < m) m = n;
-        double v[2][3], w[2][3], vp[2][3];
+    // Lanczos start vector (src/hydrodynamics.cpp:156-170): the normalised
+    // warm-start cache, or the normalised default seed when cold or when the
+    // cache is zero.
+    __device__ void start_vector(bool warm, const double* cache, double (&v)[2][3]) const {
+        double nv2 = 0.0;
         if (warm) {
             load(cache, v);
-            double nv2 = sqrt(dot(v, v));
-            if (!(nv2 > 0.0)) {
-                load(a.seed_table, v);
-                nv2 = ch.seed_norm;
-            }
-            const double inv = 1.0 / nv2;
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) v[q][d] *= inv;
-        } else {
-            load(a.seed_table, v);
-            const double inv = 1.0 / ch.seed_norm;
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) v[q][d] *= inv;
+            nv2 = sqrt(dot(v, v));
         }
+        if (!(nv2 > 0.0)) {
+            load(a.seed_table, v);
+            nv2 = ch.seed_norm;
+        }
+        const double inv = 1.0 / nv2;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) v[q][d] *= inv;
+    }
+
+    // Returns the number of Lanczos steps; sets rmin/rmax and the Ritz vectors.
+    // v0: the start vector; if have_dv0, dv0 = D v0 (computed by the caller
+    // together with the step's other independent products).
+    __device__ int lanczos(int m, bool warm, const double (&v0)[2][3], const double (&dv0)[2][3], bool have_dv0,
+                           double (&vmin)[2][3], double (&vmax)[2][3], double& rmin, double& rmax) {
+        if (n < m) m = n;
+        double v[2][3], w[2][3], vp[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) v[q][d] = v0[q][d];
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
@@ -693,30 +721,75 @@ struct TeamChain {
         int k = 0;
         double b = 0.0;
         if (m <= kLanczosWarm) {
-            // warm runs: classical Gram-Schmidt against the whole basis, each
-            // pass's projections reduced together; the projection on v_j is
-            // alpha_j. A second pass runs when the first removed more than
-            // half of |w|^2 (the DGKS criterion |w'|^2 < sum c_u^2: w lost
-            // over 1/sqrt(2) of its norm to the projections).
+            // warm runs: classical Gram-Schmidt against the whole basis. One
+            // batched team sum per step gives the projections c_u = v_u.w
+            // (u <= j; c_j = alpha_j) and, in the free slot, |w|^2 before the
+            // projection, so beta^2 = |w|^2 - sum c_u^2 (Pythagoras). When the
+            // projections removed all but 1% of |w|^2 (|w'| < 0.1 |w|, the
+            // Daniel-Gragg-Kaufman-Stewart test with eta = 0.1) a second pass
+            // re-orthogonalises and beta comes from an explicit norm. The last
+            // step's beta is not needed (it is not an entry of T).
             for (int j = 0; j < m; ++j) {
                 store(basis(j, m), v);
-                apply(v, w);
-                double al = 0.0, bsq = 0.0;
-                for (int pass = 0; pass < 2; ++pass) {
-                    double c[kLanczosWarm];
+                if (j == 0 && have_dv0) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) w[q][d] = dv0[q][d];
+                } else {
+                    apply(v, w);
+                }
+                const bool last = j == m - 1;
+                double c[kLanczosWarm];
+                double ww = 0.0;
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) ww += w[q][d] * w[q][d];
+#pragma unroll
+                for (int u = 0; u < kLanczosWarm; ++u) {
+                    c[u] = (u == kLanczosWarm - 1 && j < kLanczosWarm - 1) ? ww : 0.0;
+                    if (u <= j) {
+                        const double* vu = basis(u, m);
+#pragma unroll
+                        for (int q = 0; q < 2; ++q)
+#pragma unroll
+                            for (int d = 0; d < 3; ++d)
+                                if (valid(q)) c[u] += w[q][d] * vu[3 * bead(q) + d];
+                    }
+                }
+                tsum8(c);
+                const double w0sq = c[kLanczosWarm - 1];
+                double al = 0.0, p2 = 0.0;
+#pragma unroll
+                for (int u = 0; u < kLanczosWarm; ++u) {
+                    if (u <= j) {
+                        const double* vu = basis(u, m);
+#pragma unroll
+                        for (int q = 0; q < 2; ++q)
+#pragma unroll
+                            for (int d = 0; d < 3; ++d)
+                                if (valid(q)) w[q][d] -= c[u] * vu[3 * bead(q) + d];
+                        p2 += c[u] * c[u];
+                    }
+                    if (u == j) al = c[u];
+                }
+                double bsq = w0sq - p2;
+                if (!last && !(bsq >= 0.0101 * p2)) {
+                    double c2[kLanczosWarm];
 #pragma unroll
                     for (int u = 0; u < kLanczosWarm; ++u) {
-                        c[u] = 0.0;
+                        c2[u] = 0.0;
                         if (u <= j) {
                             const double* vu = basis(u, m);
 #pragma unroll
                             for (int q = 0; q < 2; ++q)
 #pragma unroll
                                 for (int d = 0; d < 3; ++d)
-                                    if (valid(q)) c[u] += w[q][d] * vu[3 * bead(q) + d];
+                                    if (valid(q)) c2[u] += w[q][d] * vu[3 * bead(q) + d];
                         }
                     }
-                    tsum8(c);
+                    tsum8(c2);
 #pragma unroll
                     for (int u = 0; u < kLanczosWarm; ++u) {
                         if (u <= j) {
@@ -725,20 +798,15 @@ struct TeamChain {
                             for (int q = 0; q < 2; ++q)
 #pragma unroll
                                 for (int d = 0; d < 3; ++d)
-                                    if (valid(q)) w[q][d] -= c[u] * vu[3 * bead(q) + d];
+                                    if (valid(q)) w[q][d] -= c2[u] * vu[3 * bead(q) + d];
                         }
-                    }
-                    double p2 = 0.0;
-#pragma unroll
-                    for (int u = 0; u < kLanczosWarm; ++u) {
-                        if (u == j) al += c[u];
-                        if (u <= j) p2 += c[u] * c[u];
+                        if (u == j) al += c2[u];
                     }
                     bsq = dot(w, w);
-                    if (pass == 0 && bsq >= p2) break;
                 }
                 if (tid == 0) S.alpha[k] = al;
                 ++k;
+                if (last) break;
                 b = sqrt(bsq);
                 if (b < 1.0e-10) break;
                 const double ib = 1.0 / b;
@@ -752,7 +820,14 @@ struct TeamChain {
             // cold runs (first step of a call): the reference's modified Gram-Schmidt
             for (int j = 0; j < m; ++j) {
                 store(basis(j, m), v);
-                apply(v, w);
+                if (j == 0 && have_dv0) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) w[q][d] = dv0[q][d];
+                } else {
+                    apply(v, w);
+                }
                 const double al = dot(v, w);
                 if (tid == 0) S.alpha[k] = al;
                 ++k;
@@ -869,12 +944,40 @@ struct TeamChain {
 
     // spectral_bounds (src/hydrodynamics.cpp:224-264): the warm-start vector
     // lives in the chain's cache slice.
-    __device__ void bounds(double* cache, int& cache_valid, double& lmin, double& lmax) {
+    // The step's three mutually independent products against D(R) run in
+    // one pass first: D v0 (the Lanczos start vector), D X0 (the noise, for
+    // the Chebyshev series) and D A (A = Fs + Fe, the predictor's force).
+    __device__ void bounds(double* cache, int& cache_valid, double& lmin, double& lmax, const float (&X0)[2][3],
+                           const float (&A)[2][3], float (&DX0)[2][3], float (&DA)[2][3]) {
         double vmin[2][3], vmax[2][3], rmin, rmax;
         const bool can_warm = cache_valid != 0;
-        const int steps = lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, cache, vmin, vmax, rmin, rmax);
+        double v0[2][3], dv0[2][3];
+        start_vector(can_warm, cache, v0);
+        {
+            float x3[3][2][3], y3[3][2][3];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    x3[0][q][d] = (float)v0[q][d];
+                    x3[1][q][d] = X0[q][d];
+                    x3[2][q][d] = A[q][d];
+                }
+            applyK<3>(x3, y3);
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    dv0[q][d] = (double)y3[0][q][d];
+                    DX0[q][d] = y3[1][q][d];
+                    DA[q][d] = y3[2][q][d];
+                }
+        }
+        const int steps =
+            lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, v0, dv0, true, vmin, vmax, rmin, rmax);
         if (can_warm && steps < 4) {
-            lanczos(kLanczosCold, false, cache, vmin, vmax, rmin, rmax);
+            start_vector(false, cache, v0);
+            lanczos(kLanczosCold, false, v0, dv0, false, vmin, vmax, rmin, rmax);
             cnt[C_LZCOLD] += 1;
         } else {
             cnt[can_warm ? C_LZWARM : C_LZCOLD] += 1;
@@ -906,9 +1009,9 @@ struct TeamChain {
 
     // ---- Chebyshev square root, FP32 recurrence (src/hydrodynamics.cpp:267-337)
     // Returns the FD error; out = approx D^{1/2} x0.
-    __device__ double chebyshev(const float (&x0)[2][3], double lmin, double lmax, float (&out)[2][3]) {
-        float Dx0[2][3];
-        apply32(x0, Dx0);
+    // Dx0 = D x0 (computed by the caller).
+    __device__ double chebyshev(const float (&x0)[2][3], const float (&Dx0)[2][3], double lmin, double lmax,
+                                float (&out)[2][3]) {
         const double x0Dx0 = dotf(x0, Dx0);
         double Lr = sqrt(lmax / lmin) * ch.mult + 0.5;
         int L = !(Lr < 2.0e9) ? kMaxCheb : (int)Lr + 1;
@@ -1135,7 +1238,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             W.stage_pos(R);
             float Fs[2][3], Fe[2][3];
             W.forces(R, t, Fs, Fe, true);
-            float X0[2][3], dW[2][3];
+            float X0[2][3], dW[2][3], A[2][3], DF[2][3];
             W.noise(ux, iy, seed, X0);
             // brownian_step (src/mobility.cpp:58-88)
             if (!W.hi) {
@@ -1145,9 +1248,13 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                     for (int d = 0; d < 3; ++d) dW[q][d] = (float)(sqrt_dt * X0[q][d]);
             } else {
                 double lmin, lmax;
-                float bx[2][3];
-                W.bounds(gcache, cache_valid, lmin, lmax);
-                const double fd = W.chebyshev(X0, lmin, lmax, bx);
+                float bx[2][3], DX0[2][3];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) A[q][d] = Fs[q][d] + Fe[q][d];
+                W.bounds(gcache, cache_valid, lmin, lmax, X0, A, DX0, DF);
+                const double fd = W.chebyshev(X0, DX0, lmin, lmax, bx);
                 if (!(fd <= ch.fd_tol)) {
                     W.status |= BDCU_ST_CHEB_FALLBACK;
                     W.cnt[C_FALLBACK] += 1;
@@ -1165,13 +1272,12 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             double K1[9], K2[9];
             kappa_at(ch, a.arena, t, K1);
             kappa_at(ch, a.arena, t + dt, K2);
-            float A[2][3], DF[2][3];
             double Rp[2][3];
+            if (!W.hi)  // without HI D = I; with HI, bounds() formed D (Fs + Fe)
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < 2; ++q)
 #pragma unroll
-                for (int d = 0; d < 3; ++d) A[q][d] = Fs[q][d] + Fe[q][d];
-            W.applyF(A, DF);
+                    for (int d = 0; d < 3; ++d) DF[q][d] = Fs[q][d] + Fe[q][d];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
 #pragma unroll
