@@ -245,6 +245,8 @@ def load_library():
                                     c_double_p, ctypes.c_int64]
     lib.bdcu_count_steps.argtypes = [ctypes.POINTER(BdcuSim), c_int64_p]
     lib.bdcu_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
+    lib.bdcu_run_slice.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                   vp, vp]
     lib.bdcu_integrate_host.argtypes = [vp, c_double_p, c_int32_p, c_int32_p,
                                         ctypes.POINTER(BdcuCounters), ctypes.c_int]
     lib.bdcu_total_force.argtypes = [vp, vp, vp]

@@ -446,6 +446,9 @@ struct State {
     const int32_t* n_steps;
     int32_t* status;
     bdcu_counters* counters;
+    int64_t budget_ns = 0;       // time slice (bdcu_run_slice), 0: none
+    int32_t* steps_done = nullptr;
+    double* t_end = nullptr;
 };
 
 int launch_bucket(bdcu_ctx* ctx, int form, const Bucket& b, const State& st, int cache_mode, cudaStream_t s) {
@@ -477,6 +480,9 @@ int launch_bucket(bdcu_ctx* ctx, int form, const Bucket& b, const State& st, int
     a.scratch_stride = b.scratch_stride;
     a.xs_pow = ctx->xs_pow_d;
     a.a_pow = ctx->a_pow_d;
+    a.budget_ns = st.budget_ns;
+    a.steps_done = st.steps_done;
+    a.t_end = st.t_end;
     cudaError_t e;
     if (b.kernel == BDCU_KERNEL_TEAM)
         e = launch_mixed_team(b.team_warps, a, b.grid, b.smem, s);
@@ -632,6 +638,31 @@ int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache, int32_t* cac
     int rc = build_plan(ctx, form);
     if (rc) return rc;
     const State st{R, rng, cache, cache_valid, t_start, n_steps, status, counters};
+    return run_plan(ctx, form, st, cache_mode);
+}
+
+int bdcu_run_slice(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache, int32_t* cache_valid,
+                   const double* t_start, const int32_t* n_steps, int32_t* status, bdcu_counters* counters,
+                   int form, int cache_mode, int64_t budget_ns, int32_t* steps_done, double* t_end) {
+    if (!ctx) return BDCU_E_ARG;
+    if (budget_ns < 0) return fail(ctx, BDCU_E_ARG, "negative time budget");
+    if (!steps_done || !t_end) return fail(ctx, BDCU_E_ARG, "null steps_done or t_end");
+    if (ctx->n_chains < 1) return fail(ctx, BDCU_E_STATE, "bdcu_run_slice before bdcu_set_chains or bdcu_reserve");
+    if (!R || !rng || !cache || !cache_valid || !t_start || !n_steps || !status || !counters)
+        return fail(ctx, BDCU_E_ARG, "null device pointer");
+    if (form != BDCU_FORM_PLAIN_FP64 && form != BDCU_FORM_MIXED_FP32) return fail(ctx, BDCU_E_ARG, "unknown form");
+    if (cache_mode != BDCU_CACHE_RESET_PER_CALL && cache_mode != BDCU_CACHE_PERSIST)
+        return fail(ctx, BDCU_E_ARG, "unknown cache mode");
+    CK(cudaSetDevice(ctx->device));
+    int rc = build_plan(ctx, form);
+    if (rc) return rc;
+    // chains the selection does not advance, or that are skipped (failed),
+    // report no steps
+    CK(cudaMemsetAsync(steps_done, 0, sizeof(int32_t) * (size_t)ctx->n_chains, ctx->stream));
+    State st{R, rng, cache, cache_valid, t_start, n_steps, status, counters};
+    st.budget_ns = budget_ns;
+    st.steps_done = steps_done;
+    st.t_end = t_end;
     return run_plan(ctx, form, st, cache_mode);
 }
 

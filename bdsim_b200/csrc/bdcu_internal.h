@@ -76,7 +76,20 @@ struct RunArgs {
     int64_t scratch_stride; // doubles per CTA (per team)
     const uint32_t* xs_pow; // xorshift step matrix powers: columns of M^k, 32 words per k
     const uint32_t* a_pow;  // 16807^k mod (2^31 - 1)
+    // time slice (bdcu_run_slice): a chain starts no new step once budget_ns
+    // have passed since its thread block started (0: no budget); steps_done[c]
+    // and t_end[c] (nullable) receive the steps it completed and its time.
+    int64_t budget_ns;
+    int32_t* steps_done;
+    double* t_end;
 };
+
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t v;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+    return v;
+}
 
 static_assert(sizeof(DevChain) % 8 == 0, "records are copied as doubles");
 

@@ -25,12 +25,21 @@ namespace bdcu {
 
 constexpr int kSlots = 16;     // n-vectors in shared memory
 constexpr int kCoefCap = 504;  // >= kMaxCheb + 1
+// Blocked Cholesky (3N >= kBlockedCholMin): panels of up to kCholMaxPanel
+// columns, trailing update in kCholTile x kCholTile tiles whose panel rows are
+// staged in shared memory with row stride kCholTileStride (padded against
+// bank conflicts), in vector slots kCholFirstSlot.. (free while D is factored).
+constexpr int kBlockedCholMin = 300;
+constexpr int kCholTile = 64;
+constexpr int kCholTileStride = kCholTile + 8;
+constexpr int kCholMaxPanel = 32;  // panel rows are solved with the panel in registers
+constexpr int kCholFirstSlot = 7;
 
 // Block-shared control state.
 struct Ctl {
     double com[3];
     double lmin, lmax, x0Dx0, fd_err, incr, rmin, rmax, glo, ghi, nv, bval;
-    int32_t chain, k, L, status, cache_valid, lz_steps, brk, pad;
+    int32_t chain, k, L, status, cache_valid, lz_steps, brk, stop;
     int64_t cnt[8];  // bdcu_counters order
 };
 enum { C_STEPS = 0, C_DX, C_CHEB, C_CORR, C_LZCOLD, C_LZWARM, C_FALLBACK, C_NONCONV };
@@ -226,6 +235,8 @@ struct Block {
     double* D;         // plain: dense D (shared or global)
     int ldd;
     double* Lt;        // transposed Cholesky factor, global scratch (ld = n)
+    double* stage;     // blocked Cholesky tile staging (vector slots kCholFirstSlot..)
+    int64_t stage_cap; // doubles available at stage
     float4* pos32;     // mixed: FP32 bead coordinates
     float4* vec32;     // mixed: FP32 staged vector
     int ldv;           // stride of Lanczos basis vectors
@@ -332,6 +343,8 @@ struct Block {
     // M(i,j) - L(i,0)L(j,0) - L(i,1)L(j,1) - ... in k order, then / L(j,j):
     // the reference's rounding sequence. Returns false on a pivot <= 0.
     // src: dense D at (Dp, ld) or, if src_in_lt, Lt already holds D's lower part.
+    // From 3N = kBlockedCholMin the factorisation is blocked (cholesky_blocked);
+    // vector slots kCholFirstSlot.. must then be free (the callers' are).
     __device__ bool cholesky(const double* Dp, int ld, bool src_in_lt) {
         double* L = Lt;
         if (!src_in_lt) {
@@ -339,6 +352,8 @@ struct Block {
                 for (int i = j + (threadIdx.x & 31); i < n; i += 32) L[(int64_t)j * n + i] = Dp[(int64_t)i * ld + j];
         }
         __syncthreads();
+        const int nb = chol_panel_width();
+        if (nb > 0) return cholesky_blocked(nb);
         for (int k = 0; k < n; ++k) {
             if (threadIdx.x == 0) {
                 const double s = L[(int64_t)k * n + k];
@@ -358,6 +373,185 @@ struct Block {
             __syncthreads();
         }
         return true;
+    }
+
+    // Panel width of the blocked factorisation (0: unblocked): up to
+    // kCholMaxPanel columns, a multiple of 8, such that two staged tiles of
+    // panel rows fit the staging area.
+    __device__ int chol_panel_width() const {
+        if (n < kBlockedCholMin || stage == nullptr) return 0;
+        int64_t nb = stage_cap / (2 * kCholTileStride);
+        nb = nb > kCholMaxPanel ? kCholMaxPanel : nb;
+        nb &= ~7;
+        return nb >= 8 ? (int)nb : 0;
+    }
+
+    // Blocked right-looking Cholesky. For each panel of nb columns [kb, ke):
+    // (1) the panel's diagonal block is factored in shared memory column by
+    //     column (pivot, scale, then the block's remaining columns updated);
+    //     each row below it is then solved by one thread, its nb panel
+    //     entries in registers: L(i,j) = (A(i,j) - sum_{k<j} L(i,k) L(j,k)) /
+    //     L(j,j) for j = kb, kb+1, ... in order;
+    // (2) the trailing lower triangle [ke, n)^2 is updated by the panel,
+    //     C(i,j) -= sum_{k in [kb,ke)} L(i,k) L(j,k), tile by tile, with the
+    //     tile's panel rows staged in shared memory.
+    // Every element still receives its products in k order before its
+    // division, so the plain form keeps the reference's rounding sequence
+    // (trailing update one rounded product and one rounded subtraction per
+    // k); the mixed form's trailing update runs on the FP64 tensor cores
+    // (mma.m8n8k4, products accumulated in the tensor core's own order).
+    __device__ bool cholesky_blocked(int nb) {
+        double* L = Lt;
+        double* As = stage;                          // As[k*TS + r] = L(i0 + r, kb + k)
+        double* Bs = stage + (int64_t)nb * kCholTileStride;  // Bs[k*TS + c] = L(j0 + c, kb + k)
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        for (int kb = 0; kb < n; kb += nb) {
+            const int ke = kb + nb < n ? kb + nb : n;
+            if (!chol_panel(kb, ke)) return false;
+            if (ke >= n) break;
+            const int kk = ke - kb;
+            const int mt = (n - ke + kCholTile - 1) / kCholTile;
+            for (int tt = 0; tt < mt * (mt + 1) / 2; ++tt) {
+                int ti = (int)((sqrt(8.0 * tt + 1.0) - 1.0) * 0.5);
+                while (ti * (ti + 1) / 2 > tt) --ti;
+                while ((ti + 1) * (ti + 2) / 2 <= tt) ++ti;
+                const int tj = tt - ti * (ti + 1) / 2;  // tile (ti, tj), tj <= ti
+                const int i0 = ke + ti * kCholTile, j0 = ke + tj * kCholTile;
+                for (int e = threadIdx.x; e < nb * kCholTile; e += blockDim.x) {
+                    const int k = e / kCholTile, r = e % kCholTile;
+                    const bool kin = k < kk;
+                    As[k * kCholTileStride + r] = (kin && i0 + r < n) ? L[(int64_t)(kb + k) * n + i0 + r] : 0.0;
+                    Bs[k * kCholTileStride + r] = (kin && j0 + r < n) ? L[(int64_t)(kb + k) * n + j0 + r] : 0.0;
+                }
+                __syncthreads();
+                if constexpr (!kMixed) chol_tile_simt(As, Bs, i0, j0, kk);
+                else chol_tile_dmma(As, Bs, i0, j0, (kk + 3) & ~3, warp, lane, nwarps);
+                __syncthreads();
+            }
+        }
+        return true;
+    }
+
+    // Panel [kb, ke) of the blocked factorisation (step 1 above). The
+    // diagonal block is staged column-major in shared memory (stage);
+    // returns false on a pivot <= 0.
+    __device__ bool chol_panel(int kb, int ke) {
+        double* L = Lt;
+        const int kk = ke - kb;
+        double* D11 = stage;  // D11[c * kk + r] = L(kb + r, kb + c), r >= c
+        for (int e = threadIdx.x; e < kk * kk; e += blockDim.x) {
+            const int r = e % kk, c = e / kk;
+            D11[e] = r >= c ? L[(int64_t)(kb + c) * n + kb + r] : 0.0;
+        }
+        __syncthreads();
+        for (int k = 0; k < kk; ++k) {
+            if (threadIdx.x == 0) {
+                const double s = D11[k * kk + k];
+                if (!(s > 0.0)) ctl.brk = 1; else D11[k * kk + k] = sqrt(s);
+            }
+            __syncthreads();
+            if (ctl.brk) return false;
+            const double dk = D11[k * kk + k];
+            for (int r = k + 1 + threadIdx.x; r < kk; r += blockDim.x) D11[k * kk + r] = D11[k * kk + r] / dk;
+            __syncthreads();
+            for (int e = threadIdx.x; e < kk * kk; e += blockDim.x) {
+                const int r = e % kk, j = e / kk;
+                if (j > k && r >= j) D11[j * kk + r] = D11[j * kk + r] - D11[k * kk + r] * D11[k * kk + j];
+            }
+            __syncthreads();
+        }
+        for (int e = threadIdx.x; e < kk * kk; e += blockDim.x) {
+            const int r = e % kk, c = e / kk;
+            if (r >= c) L[(int64_t)(kb + c) * n + kb + r] = D11[e];
+        }
+        // rows below the block, one per thread
+        for (int i = ke + threadIdx.x; i < n; i += blockDim.x) {
+            double a[kCholMaxPanel];
+#pragma unroll
+            for (int k = 0; k < kCholMaxPanel; ++k) a[k] = k < kk ? L[(int64_t)(kb + k) * n + i] : 0.0;
+#pragma unroll
+            for (int j = 0; j < kCholMaxPanel; ++j) {
+                if (j < kk) {
+                    double s = a[j];
+#pragma unroll
+                    for (int k = 0; k < j; ++k) s = s - a[k] * D11[k * kk + j];
+                    a[j] = s / D11[j * kk + j];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kCholMaxPanel; ++k)
+                if (k < kk) L[(int64_t)(kb + k) * n + i] = a[k];
+        }
+        __syncthreads();
+        return true;
+    }
+
+    // Trailing-update tile, FP64 CUDA cores: 4x4 elements per thread, each
+    // element c = c - a_k * b_k for k = 0, 1, ... (no contraction: the plain
+    // form is compiled without FMA).
+    __device__ void chol_tile_simt(const double* As, const double* Bs, int i0, int j0, int kk) {
+        double* L = Lt;
+        constexpr int Q = kCholTile / 4;
+        for (int mtl = threadIdx.x; mtl < Q * Q; mtl += blockDim.x) {
+            const int r0 = (mtl % Q) * 4, c0 = (mtl / Q) * 4;
+            if (i0 + r0 + 3 < j0 + c0) continue;  // all above the diagonal
+            double c[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int i = i0 + r0 + u, j = j0 + c0 + v;
+                    c[u][v] = (i < n && j < n && i >= j) ? L[(int64_t)j * n + i] : 0.0;
+                }
+            for (int k = 0; k < kk; ++k) {
+                const double2 a01 = *reinterpret_cast<const double2*>(As + k * kCholTileStride + r0);
+                const double2 a23 = *reinterpret_cast<const double2*>(As + k * kCholTileStride + r0 + 2);
+                const double2 b01 = *reinterpret_cast<const double2*>(Bs + k * kCholTileStride + c0);
+                const double2 b23 = *reinterpret_cast<const double2*>(Bs + k * kCholTileStride + c0 + 2);
+                const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) c[u][v] = c[u][v] - av[u] * bv[v];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int i = i0 + r0 + u, j = j0 + c0 + v;
+                    if (i < n && j < n && i >= j) L[(int64_t)j * n + i] = c[u][v];
+                }
+        }
+    }
+
+    // Trailing-update tile on the FP64 tensor cores: the tile is 8x8 blocks
+    // of 8x8; warp w takes blocks w, w + nwarps, ...; each block is
+    // C += (-A) B over k in steps of 4 with mma.sync.m8n8k4.f64 (A 8x4 row:
+    // lane holds A[lane/4][lane%4]; B 4x8 col: lane holds B[lane%4][lane/4];
+    // C 8x8: lane holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]).
+    // kk4: the panel width rounded up to 4 (the staged rows are zero beyond).
+    __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int kk4, int warp, int lane,
+                                   int nwarps) {
+        double* L = Lt;
+        constexpr int B8 = kCholTile / 8;
+        const int g = lane >> 2, q = lane & 3;
+        for (int blk = warp; blk < B8 * B8; blk += nwarps) {
+            const int tr = (blk % B8) * 8, tc = (blk / B8) * 8;
+            if (i0 + tr + 7 < j0 + tc) continue;  // all above the diagonal
+            const int i = i0 + tr + g, ja = j0 + tc + 2 * q, jb = ja + 1;
+            const bool oka = i < n && ja < n && i >= ja, okb = i < n && jb < n && i >= jb;
+            double c0 = oka ? L[(int64_t)ja * n + i] : 0.0;
+            double c1 = okb ? L[(int64_t)jb * n + i] : 0.0;
+            for (int k = 0; k < kk4; k += 4) {
+                const double av = -As[(k + q) * kCholTileStride + tr + g];
+                const double bv = Bs[(k + q) * kCholTileStride + tc + g];
+                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                             : "+d"(c0), "+d"(c1)
+                             : "d"(av), "d"(bv));
+            }
+            if (oka) L[(int64_t)ja * n + i] = c0;
+            if (okb) L[(int64_t)jb * n + i] = c1;
+        }
     }
 
     // y = L x (lower_matvec, src/linalg.cpp:109-117), row sums in j order.
@@ -729,10 +923,13 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
     B.Vg = scr + scl.V;
     B.ldv = nvs;
     B.Lt = scr + scl.Lt;
+    B.stage = B.slot[kCholFirstSlot];
+    B.stage_cap = (int64_t)(kSlots - kCholFirstSlot) * nvs;
     B.pos32 = reinterpret_cast<float4*>(sm + lay.f32);
     B.vec32 = reinterpret_cast<float4*>(sm + lay.f32 + nvs);
 
     const int tid = threadIdx.x;
+    const uint64_t t_launch = global_ns();
     for (;;) {
         if (tid == 0) {
             const int item = atomicAdd(a.work_counter, 1);
@@ -806,7 +1003,13 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
         const double sqrt_dt = sqrt(dt);
         __syncthreads();
 
-        for (int step = 0; step < nsteps; ++step) {
+        int step = 0;
+        for (; step < nsteps; ++step) {
+            if (a.budget_ns > 0) {  // time slice: no new step past the budget
+                if (tid == 0) ctl.stop = (int64_t)(global_ns() - t_launch) >= a.budget_ns;
+                __syncthreads();
+                if (ctl.stop) break;
+            }
             // recenter (src/integrator.cpp:88-93)
             if (ch.update_com) {
                 if (tid < 3) {
@@ -1065,6 +1268,8 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             a.status[c] = ctl.status;
             int64_t* cc = reinterpret_cast<int64_t*>(a.counters + c);
             for (int k = 0; k < 8; ++k) cc[k] += ctl.cnt[k];
+            if (a.steps_done) a.steps_done[c] = step;
+            if (a.t_end) a.t_end[c] = t;
         }
         __syncthreads();
     }

@@ -1157,6 +1157,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
     const int64_t gw = (int64_t)blockIdx.x * TeamCfg<T>::kTeamsPerCta + team;
     double* scr = a.scratch + gw * a.scratch_stride;
     const int nvr = (int)round_up8(a.n_max);
+    const uint64_t t_launch = global_ns();
 
     for (;;) {
         if (tid == 0) {
@@ -1220,7 +1221,10 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
         const double dt = ch.dt;
         const double sqrt2inv = 1.0 / sqrt(2.0);
         const double sqrt_dt = sqrt(dt);
-        for (int step = 0; step < nsteps; ++step) {
+        int step = 0;
+        for (; step < nsteps; ++step) {
+            // time slice: no new step past the budget (thread 0 decides for the team)
+            if (a.budget_ns > 0 && W.tor(tid == 0 && (int64_t)(global_ns() - t_launch) >= a.budget_ns)) break;
             // recenter (src/integrator.cpp:88-93)
             if (ch.update_com) {
                 double com[3];
@@ -1484,6 +1488,8 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             a.status[c] = W.status;
             int64_t* cc = reinterpret_cast<int64_t*>(a.counters + c);
             for (int k = 0; k < 8; ++k) cc[k] += (int64_t)W.cnt[k];
+            if (a.steps_done) a.steps_done[c] = step;
+            if (a.t_end) a.t_end[c] = t;
         }
         team_sync<T>(team);
     }

@@ -90,6 +90,16 @@ class Context:
                                    dptr(n_steps), dptr(status), dptr(counters), int(form), int(cache_mode)),
                  "bdcu_run")
 
+    def run_slice(self, R, rng, cache, cache_valid, t_start, n_steps, status, counters, form, cache_mode,
+                  budget_ns, steps_done, t_end):
+        """bdcu_run with a time budget: steps_done / t_end receive each chain's
+        completed steps and time (see bdcu_run_slice)."""
+        self.use_stream()
+        self._ck(self.lib.bdcu_run_slice(self.h, dptr(R), dptr(rng), dptr(cache), dptr(cache_valid),
+                                         dptr(t_start), dptr(n_steps), dptr(status), dptr(counters), int(form),
+                                         int(cache_mode), int(budget_ns), dptr(steps_done), dptr(t_end)),
+                 "bdcu_run_slice")
+
     def integrate_host(self, R_host: np.ndarray, rng_host: np.ndarray, form):
         """Host-buffer integrate over each chain's SimParams span (cold cache).
         R_host (total_beads, 3) float64 and rng_host (n, 3) int32 are updated

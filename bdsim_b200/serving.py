@@ -8,16 +8,24 @@ admits jobs -- each the arguments of a `simulate` call -- while others run:
     slots, n_traj*N consecutive beads of the pool (the pool is the HBM budget:
     positions, warm-start vectors and the snapshot buffers) and room under the
     active-chain cap; queued jobs are admitted in arrival order with a short
-    first-fit lookahead, and arrivals beyond the queue limit are rejected;
-  * each server iteration advances every running job by one chunk
-    (write_every steps, the job's snapshot interval) in ONE bdcu_run over all
-    their chains (buckets by bead count, device work lists), so jobs of
-    different N, n_traj and n_steps share the GPU;
-  * after each chunk the positions are copied on the device to a snapshot
-    buffer and from there to pinned host memory on a copy stream while the
-    next chunk runs; the host delivers each job's snapshot (and, at its last
-    step, its statuses) one iteration later and frees the slots of finished
-    jobs for the next admission;
+    first-fit lookahead (policy "fifo") or smallest estimated work first
+    (policy "sjf": n_traj * n_steps * N^2, the pair work of its D.x products),
+    and arrivals beyond the queue limit are rejected;
+  * each server iteration is ONE time-sliced launch (bdcu_run_slice) over the
+    chains of every running job (buckets by bead count, device work lists),
+    so jobs of different N, n_traj and n_steps share the GPU: every chain
+    takes up to `slice_steps` steps of its current chunk (write_every steps,
+    the job's snapshot interval), and none starts a new step after
+    `slice_budget_s` -- a job whose steps are slow (a corrector at its
+    100N-iteration cap takes ~1 s per step at N=300) cannot hold the others'
+    snapshots back;
+  * the launch reports each chain's completed steps and time; a chunk in
+    progress continues in the next launch from there with its warm spectral
+    cache, so a chunk cut into slices gives the same chains, bit for bit, as
+    one integrate call over it;
+  * when all of a job's chains have finished a chunk, its positions are
+    copied to the host and delivered (at its last chunk with its statuses),
+    and a finished job's slots are freed for the next admission;
   * latency of a job = arrival to delivery of its last snapshot.
 
 A job's chains follow exactly the trajectory of `simulate` with the same
@@ -34,7 +42,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._abi import CACHE_RESET_PER_CALL, COUNTER_FIELDS, ST_FATAL_MASK, count_steps
+from ._abi import CACHE_PERSIST, CACHE_RESET_PER_CALL, COUNTER_FIELDS, ST_FATAL_MASK, count_steps
 from .engine import Context, _torch, form_code
 from .ensemble import INITIALIZERS, Initial, _segment, n_steps_of
 from .params import PhysParams, Rng, SimParams
@@ -106,7 +114,9 @@ class JobState:
     t_admit: float = None
     t_done: float = None
     n_steps: int = 0
-    step: int = 0  # steps enqueued on the device
+    step: int = 0  # steps of the chunks completed
+    chunk_end: int = -1  # step count at the end of the chunk in progress (-1: none)
+    t_chunk_end: float = 0.0
     slot0: int = -1
     bead0: int = -1
     arena0: int = -1
@@ -138,11 +148,17 @@ class Server:
     def __init__(self, device: int = 0, form="mixed", max_chains: int = 65536, bead_capacity: int = None,
                  hbm_budget_bytes: int = 1 << 30, arena_capacity: int = 1 << 20, max_active_chains: int = None,
                  queue_limit: int = None, lookahead: int = 16, cache_mode: int = CACHE_RESET_PER_CALL,
-                 on_snapshot=None, clock=time.monotonic):
+                 on_snapshot=None, clock=time.monotonic, slice_steps: int = 10, slice_budget_s: float = 1.0,
+                 policy: str = "fifo"):
         torch = _torch()
         self.torch = torch
         self.form = form_code(form)
         self.cache_mode = cache_mode
+        if policy not in ("fifo", "sjf"):
+            raise ValueError("policy is 'fifo' or 'sjf'")
+        self.policy = policy
+        self.slice_steps = int(slice_steps)
+        self.budget_ns = int(slice_budget_s * 1e9)
         self.clock = clock
         self.on_snapshot = on_snapshot
         self.max_chains = int(max_chains)
@@ -163,14 +179,16 @@ class Server:
         self.counters = torch.zeros((nc, len(COUNTER_FIELDS)), dtype=torch.int64, device=dev)
         self.t0 = torch.zeros(nc, dtype=torch.float64, device=dev)
         self.k = torch.zeros(nc, dtype=torch.int32, device=dev)
-        self.snap = [torch.zeros((nb, 3), dtype=torch.float64, device=dev) for _ in range(2)]
-        self.snap_host = [torch.empty((nb, 3), dtype=torch.float64, pin_memory=True) for _ in range(2)]
-        self.status_host = [torch.empty(nc, dtype=torch.int32, pin_memory=True) for _ in range(2)]
-        self.tk_host = [(torch.zeros(nc, dtype=torch.float64, pin_memory=True),
-                         torch.zeros(nc, dtype=torch.int32, pin_memory=True)) for _ in range(2)]
-        self.tk_event = [None, None]
-        self.d2h_event = [None, None]
-        self.copy_stream = torch.cuda.Stream(device=dev)
+        self.steps_done = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self.t_end = torch.zeros(nc, dtype=torch.float64, device=dev)
+        # host view of every slot: steps left in its chunk, time of its next step
+        self.rem = np.zeros(nc, dtype=np.int32)
+        self.tnext = np.zeros(nc, dtype=np.float64)
+        self.t_host = torch.zeros(nc, dtype=torch.float64, pin_memory=True)
+        self.k_host = torch.zeros(nc, dtype=torch.int32, pin_memory=True)
+        self.done_host = torch.zeros(nc, dtype=torch.int32, pin_memory=True)
+        self.tend_host = torch.zeros(nc, dtype=torch.float64, pin_memory=True)
+        self.status_host = torch.zeros(nc, dtype=torch.int32, pin_memory=True)
         self.slots = Intervals(nc)
         self.beads = Intervals(nb)
         self.arena = Intervals(arena_capacity)
@@ -178,7 +196,6 @@ class Server:
         self.running: list[JobState] = []
         self.done: list[JobState] = []
         self.rejected: list[JobState] = []
-        self._pending = None  # (parity, manifest) of the chunk whose snapshot is in flight
         self._iter = 0
         self._selected = None
         self.active_chains = 0
@@ -206,15 +223,15 @@ class Server:
         return js
 
     def busy(self) -> bool:
-        return bool(self.queue or self.running or self._pending)
+        return bool(self.queue or self.running)
 
     def step(self):
-        """One server iteration: admit, enqueue one chunk of every running job,
-        deliver the previous chunk's snapshots."""
+        """One server iteration: admit, one time-sliced launch over the
+        running jobs, deliver the chunks it completed."""
         self._admit()
-        launched = self._launch_chunk()
-        self._deliver()  # the chunk before: its copy ran while this one was queued
-        self._pending = launched
+        work = self._launch_slice()
+        if work is not None:
+            self._finish_slice(*work)
 
     def run_until_idle(self, max_iters: int = 10 ** 9):
         it = 0
@@ -249,7 +266,9 @@ class Server:
         lat = np.array([j.latency for j in self.done], dtype=np.float64)
         svc = np.array([j.t_done - j.t_admit for j in self.done], dtype=np.float64)
         t0 = self.t_first if t0 is None else t0
-        wall = (max(j.t_done for j in self.done) - t0) if self.done else 0.0
+        # throughput over the whole replay: up to the last completion, or up
+        # to now when nothing has completed yet
+        wall = ((max(j.t_done for j in self.done) if self.done else self.clock()) - t0) if t0 is not None else 0.0
         pct = (lambda a, q: float(np.percentile(a, q)) if a.size else None)
         return {"jobs_completed": len(self.done), "jobs_rejected": len(self.rejected),
                 "jobs_queued": len(self.queue), "jobs_running": len(self.running),
@@ -262,8 +281,11 @@ class Server:
 
     def _admit(self):
         torch = self.torch
+        if self.policy == "sjf" and len(self.queue) > 1:
+            self.queue.sort(key=lambda q: (int(q.job.n_traj) * q.n_steps * q.n_beads ** 2, q.t_arrival))
         i, looked = 0, 0
-        while i < len(self.queue) and looked < self.lookahead:
+        limit = self.lookahead if self.policy == "fifo" else len(self.queue)
+        while i < len(self.queue) and looked < limit:
             js = self.queue[i]
             job = js.job
             n, N = int(job.n_traj), js.n_beads
@@ -305,80 +327,82 @@ class Server:
             self.active_chains += n
             self.running.append(js)
 
-    def _launch_chunk(self):
+    def _launch_slice(self):
         torch = self.torch
-        work = [js for js in self.running if js.step < js.n_steps]
+        work = [js for js in self.running if js.state == "running"]
         if not work:
             return None
-        par = self._iter & 1
         self._iter += 1
-        if self.tk_event[par] is not None:
-            self.tk_event[par].synchronize()
-        th, kh = self.tk_host[par]
-        tn, kn = th.numpy(), kh.numpy()
-        manifest, sel = [], []
+        rem, tnext = self.rem, self.tnext
+        fresh = []
         for js in work:
-            job, n = js.job, int(js.job.n_traj)
-            sim = job.sim
-            w = job.write_every if (job.write_every and job.write_every > 0) else js.n_steps
-            chunk = min(w, js.n_steps - js.step)
-            t0 = sim.time_start + js.step * sim.dt
-            k = count_steps(_segment(sim, t0, t0 + (chunk - 1) * sim.dt))
-            tn[js.slot0:js.slot0 + n] = t0
-            kn[js.slot0:js.slot0 + n] = k
-            sel.extend(range(js.slot0, js.slot0 + n))
-            js.step += chunk
-            self.chain_steps += n * k
-            manifest.append((js, js.step, sim.time_start + js.step * sim.dt, js.step >= js.n_steps))
-        hi_slot = max(js.slot0 + js.job.n_traj for js in work)
-        self.t0[:hi_slot].copy_(th[:hi_slot], non_blocking=True)
-        self.k[:hi_slot].copy_(kh[:hi_slot], non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record()
-        self.tk_event[par] = ev
+            if js.chunk_end < 0:  # start the job's next chunk: one integrate span
+                job, n, sim = js.job, int(js.job.n_traj), js.job.sim
+                w = job.write_every if (job.write_every and job.write_every > 0) else js.n_steps
+                chunk = min(w, js.n_steps - js.step)
+                t0 = sim.time_start + js.step * sim.dt
+                k = count_steps(_segment(sim, t0, t0 + (chunk - 1) * sim.dt))
+                rem[js.slot0:js.slot0 + n] = k
+                tnext[js.slot0:js.slot0 + n] = t0
+                js.chunk_end = js.step + chunk
+                js.t_chunk_end = sim.time_start + js.chunk_end * sim.dt
+                fresh.append((js.slot0, n))
+        sel = [s for js in work for s in range(js.slot0, js.slot0 + int(js.job.n_traj)) if rem[s] > 0]
+        if not sel:
+            return work, []
+        hi_slot = max(js.slot0 + int(js.job.n_traj) for js in work)
+        kh = self.k_host.numpy()
+        kh[:hi_slot] = np.minimum(rem[:hi_slot], self.slice_steps)
+        self.t_host.numpy()[:hi_slot] = tnext[:hi_slot]
+        self.t0[:hi_slot].copy_(self.t_host[:hi_slot], non_blocking=True)
+        self.k[:hi_slot].copy_(self.k_host[:hi_slot], non_blocking=True)
+        if self.cache_mode == CACHE_RESET_PER_CALL:
+            for s0, n in fresh:  # a new chunk starts with a cold spectral cache (a new integrate call)
+                self.valid[s0:s0 + n].zero_()
         key = tuple(sel)
         if key != self._selected:
             self.ctx.select(sel)
             self._selected = key
-        self.ctx.run(self.R, self.rng, self.cache, self.valid, self.t0, self.k, self.status, self.counters,
-                     self.form, self.cache_mode)
-        hw = max(js.bead0 + js.job.n_traj * js.n_beads for js in work)
-        if self.d2h_event[par] is not None:
-            self.d2h_event[par].synchronize()  # the host buffer of two chunks ago is delivered
-        snap, host = self.snap[par], self.snap_host[par]
-        snap[:hw].copy_(self.R[:hw])
-        st_host = self.status_host[par]
-        done_copy = torch.cuda.Event()
-        done_copy.record()
-        with torch.cuda.stream(self.copy_stream):
-            self.copy_stream.wait_event(done_copy)
-            host[:hw].copy_(snap[:hw], non_blocking=True)
-            st_host[:hi_slot].copy_(self.status[:hi_slot], non_blocking=True)
-            ev2 = torch.cuda.Event()
-            ev2.record(self.copy_stream)
-        self.d2h_event[par] = ev2
-        return (par, manifest)
+        self.ctx.run_slice(self.R, self.rng, self.cache, self.valid, self.t0, self.k, self.status, self.counters,
+                           self.form, CACHE_PERSIST, self.budget_ns, self.steps_done, self.t_end)
+        self.done_host[:hi_slot].copy_(self.steps_done[:hi_slot], non_blocking=True)
+        self.tend_host[:hi_slot].copy_(self.t_end[:hi_slot], non_blocking=True)
+        self.status_host[:hi_slot].copy_(self.status[:hi_slot], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        return work, sel, ev
 
-    def _deliver(self):
-        if self._pending is None:
-            return
-        par, manifest = self._pending
-        self._pending = None
-        self.d2h_event[par].synchronize()
-        host = self.snap_host[par].numpy()
-        sth = self.status_host[par].numpy()
+    def _finish_slice(self, work, sel, ev=None):
+        if ev is not None:
+            ev.synchronize()
+        sel = np.asarray(sel, dtype=np.int64)
+        if sel.size:
+            done = self.done_host.numpy()[sel]
+            self.rem[sel] -= done
+            moved = done > 0
+            self.tnext[sel[moved]] = self.tend_host.numpy()[sel[moved]]
+            self.chain_steps += int(done.sum())
+            fatal = (self.status_host.numpy()[sel] & ST_FATAL_MASK) != 0
+            self.rem[sel[fatal]] = 0  # a failed chain is stopped for good
         now = self.clock()
-        for js, step, t, final in manifest:
-            n, N = int(js.job.n_traj), js.n_beads
-            rows = host[js.bead0:js.bead0 + n * N].reshape(n, N, 3)
-            js.steps.append(step)
-            js.times.append(t)
+        for js in work:
+            n = int(js.job.n_traj)
+            if js.chunk_end < 0 or self.rem[js.slot0:js.slot0 + n].any():
+                continue
+            # chunk complete for every chain: deliver its snapshot
+            js.step = js.chunk_end
+            js.chunk_end = -1
+            N = js.n_beads
+            rows = self.R[js.bead0:js.bead0 + n * N].cpu().numpy().reshape(n, N, 3)
+            js.steps.append(js.step)
+            js.times.append(js.t_chunk_end)
             if js.job.keep_snapshots:
                 js.positions.append(rows.copy())
             if self.on_snapshot is not None:
-                self.on_snapshot(js, step, t, rows)
-            if final:
-                js.status = sth[js.slot0:js.slot0 + n].copy()
+                self.on_snapshot(js, js.step, js.t_chunk_end, rows)
+            st = self.status_host.numpy()[js.slot0:js.slot0 + n]
+            if js.step >= js.n_steps or bool(((st & ST_FATAL_MASK) != 0).all()):
+                js.status = st.copy()
                 js.state, js.t_done = "done", now
                 self._retire(js)
 

@@ -11,7 +11,9 @@ write_every block), i.e. one launch of the persistent integrator kernel. The
 headline value is the FP32-mixed form; the FP64 plain form is measured in the
 same run. `e2e` goes through the reference-facing host-buffer entry point
 (bdcu_integrate_host: pinned R and RNG state copied in, integrated, copied
-out every step).
+out every step). `ensemble` compares the final ensemble <Rg^2> and <tau_xy>
+of the two forms; `latency` is the p50/p99 job latency of the serving
+workload replayed against the continuous-batching server.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -42,6 +44,11 @@ DT = 1e-3
 WORKLOAD = ("4096 chains x N=50, FENE b=50, RPY h*=0.25 Chebyshev+Lanczos, Gauss EV z*=1 d*=0.5, "
             "shear 1.0, dt=1e-3, gaussian_chain(50, bond_std=1, seed=i), Rng(i)")
 METRIC = "chain-steps/sec at N=50 HI (FP32-mixed vs FP64 plain, 1 B200)"
+SERVING_WORKLOAD = ("Poisson arrivals 200 jobs/s; N ~ U{10..300}, n_traj ~ U{1..256}, n_steps log-uniform "
+                    "[1e3, 1e5], shear or uniaxial at U[0.1, 5], FENE b=100, h*=0.25 Chebyshev, write_every=100; "
+                    "replayed in real time for the horizon; shortest-job-first admission under a 256-job queue "
+                    "bound and 4096 active chains, 100-step / 1 s time slices; jobs not finished by the end of "
+                    "the horizon are not counted")
 # Flop accounting per chain-step (dense-equivalent, the same for both forms):
 #   each D.x product on the 3N-vector counts 2*(3N)^2 flops; each EV pair
 #   evaluation 20 flops (2 evaluations per step, at R and R~); RPY pair
@@ -156,8 +163,36 @@ def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream):
         stream.synchronize()
         c1 = ens.counter_totals()
         failed = int(ens.failed().sum())
+        obs = observables(ens, phys)
     delta = {k: c1[k] - c0[k] for k in c1}
-    return {"ms": times, "counters": delta, "failed": failed}
+    return {"ms": times, "counters": delta, "failed": failed, "obs": obs}
+
+
+def observables(ens, phys):
+    """Per-chain Rg^2 and Kramers shear stress tau_xy (total force computed
+    on the device, python/bdsim/properties.py:17-41) of the final state."""
+    R = np.stack(ens.positions())
+    F = np.stack(ens.total_force())
+    X = R - R.mean(axis=1, keepdims=True)
+    rg2 = np.einsum("cni,cni->c", X, X) / R.shape[1]
+    tau_xy = np.einsum("cn,cn->c", X[:, :, 0], F[:, :, 1])
+    return {"rg2": rg2, "tau_xy": tau_xy}
+
+
+def compare_observables(m, p):
+    """Ensemble means of the two forms, their standard errors, the
+    difference in units of the combined standard error, and the paired
+    (same chain, same noise) difference."""
+    out = {}
+    for k in ("rg2", "tau_xy"):
+        a, b = m[k], p[k]
+        se_a, se_b = a.std(ddof=1) / np.sqrt(a.size), b.std(ddof=1) / np.sqrt(b.size)
+        d = a - b
+        out[k] = {"mixed": float(a.mean()), "plain": float(b.mean()), "se_mixed": float(se_a),
+                  "se_plain": float(se_b),
+                  "diff_in_sigma": float((a.mean() - b.mean()) / np.sqrt(se_a ** 2 + se_b ** 2)),
+                  "paired_mean_abs_rel_diff": float(np.mean(np.abs(d)) / max(np.mean(np.abs(b)), 1e-300))}
+    return out
 
 
 def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
@@ -201,7 +236,7 @@ def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
 
 
 def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed", queue_limit=256,
-                max_active=16384, drain=False):
+                max_active=4096, drain=False, policy="sjf", slice_steps=100, slice_budget_s=1.0):
     """The serving workload: Poisson job arrivals replayed in real time
     against the continuous-batching server for `horizon` seconds. Jobs: N ~
     U{10..300}, n_traj ~ U{1..256}, n_steps log-uniform [1e3, 1e5] (times
@@ -217,12 +252,14 @@ def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed
                                 write_every=sp.write_every, keep_snapshots=False))
         arrivals.append(sp.arrival)
     srv = serving.Server(device=torch.cuda.current_device(), form=form, max_chains=max_active,
-                         hbm_budget_bytes=2 << 30, queue_limit=queue_limit, max_active_chains=max_active)
+                         hbm_budget_bytes=2 << 30, queue_limit=queue_limit, max_active_chains=max_active,
+                         policy=policy, slice_steps=slice_steps, slice_budget_s=slice_budget_s)
     torch.cuda.synchronize()
     st = srv.run_stream(jobs, np.asarray(arrivals), horizon=horizon, drain=drain)
     torch.cuda.synchronize()
     st.update({"jobs_offered": len(jobs), "horizon_s": horizon, "rate_jobs_per_s": rate,
                "n_steps_scale": scale_steps, "queue_limit": queue_limit, "max_active_chains": max_active,
+               "policy": policy, "slice_steps": slice_steps, "slice_budget_s": slice_budget_s,
                "offered_chain_steps": int(sum(j.n_traj * j.n_steps for j in jobs))})
     return st
 
@@ -283,6 +320,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg (profiling runs)")
     ap.add_argument("--chains", type=int, default=N_CHAINS, help="chains per GPU (profiling runs use fewer)")
     ap.add_argument("--forms", default="plain,mixed", help="integrator forms to time")
+    ap.add_argument("--serving-seconds", type=float, default=60.0,
+                    help="length of the serving replay (0: skip it)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -350,6 +389,9 @@ def main():
 
     e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), 1, rank * n_chains,
                                            "mixed")
+    serving = None
+    if args.serving_seconds > 0 and set(forms) == {"plain", "mixed"}:
+        serving = run_serving(torch, args.serving_seconds, seed=rank)
 
     if rank != 0:
         if dist is not None:
@@ -373,7 +415,10 @@ def main():
     launch_ms = float(np.mean(mixed["ms"]))
     peak32 = measure_peak(False)
     peak64 = measure_peak(True)
-    achieved = n_chains * CHUNK * fl_m / (launch_ms * 1e-3) / 1e12
+    # algorithmic work: the reference algorithm's products (counted by the
+    # plain form, which performs exactly those); the mixed form merges one of
+    # them by linearity, so its own count (dx_m) is lower
+    achieved = n_chains * CHUNK * fl_p / (launch_ms * 1e-3) / 1e12
     achieved_p = n_chains * CHUNK * fl_p / (float(np.mean(plain["ms"])) * 1e-3) / 1e12
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
@@ -409,7 +454,7 @@ def main():
                      "frac": achieved / peak32, "traffic": traffic,
                      "peak_source": "measured in this run: FP32 FMA-loop kernel (libbdsim_peak.so); the kernel "
                                     "runs on CUDA cores, neither HBM- nor tensor-bound",
-                     "flops_per_chain_step": fl_m, "dx_per_step": dx_m,
+                     "flops_per_chain_step": fl_p, "dx_per_step_algorithm": dx_p, "dx_per_step_mixed": dx_m,
                      "hbm_peak_gbs_measured": _peaks().get("hbm_gbs")},
         "e2e": None if e2e is None else {
             "value": e2e[0], "unit": "chain-steps/s", "h2d_bytes_per_step": e2e[1], "d2h_bytes_per_step": e2e[2],
@@ -418,6 +463,16 @@ def main():
         "clocks": clocks,
         "cpu_baseline": cpu,
         "failed_chains": {"mixed": mixed["failed"], "plain": plain["failed"]},
+        "ensemble": dict(compare_observables(mixed["obs"], plain["obs"]),
+                         steps_per_chain=(args.warmup + args.steps) * CHUNK, n_chains=n_chains,
+                         note="final state of each form from the same initial chains and seeds"),
+        "latency": None if serving is None else {
+            "p50_s": serving["p50_latency_s"], "p99_s": serving["p99_latency_s"],
+            "workload": SERVING_WORKLOAD, "under": "overload (offered load far above one GPU's capacity)",
+            **{k: serving[k] for k in ("jobs_offered", "jobs_completed", "jobs_rejected", "jobs_running",
+                                       "jobs_queued", "horizon_s", "chain_steps_per_s", "p50_service_s",
+                                       "p99_service_s", "queue_limit", "max_active_chains", "policy",
+                                       "slice_steps", "slice_budget_s")}},
     }
     print(json.dumps(line))
     if dist is not None:

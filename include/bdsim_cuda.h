@@ -204,6 +204,23 @@ int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache,
              int32_t* cache_valid, const double* t_start, const int32_t* n_steps,
              int32_t* status, bdcu_counters* counters, int form, int cache_mode);
 
+/* bdcu_run with a time slice, for serving loops that share the GPU between
+   jobs (no counterpart in the reference, whose integrate calls run to
+   completion, ChainIntegrator::run, src/integrator.cpp:101-120): a chain
+   starts no new step once budget_ns nanoseconds have passed since its thread
+   block started (0: no limit; a step in progress always completes), so one
+   slow chain (e.g. a corrector at its 100N-iteration cap) cannot hold the
+   launch for long. Per chain (device, n_chains entries, zeroed first for the
+   chains it does not advance): steps_done = steps completed, t_end = the
+   chain's time after them (the device's running sum t += dt). Continuing with
+   t_start = t_end, n_steps = the remainder and the spectral cache kept
+   (BDCU_CACHE_PERSIST, cache_valid left as the slice left it) gives the same
+   result, bit for bit, as one uninterrupted bdcu_run. */
+int bdcu_run_slice(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache,
+                   int32_t* cache_valid, const double* t_start, const int32_t* n_steps,
+                   int32_t* status, bdcu_counters* counters, int form, int cache_mode,
+                   int64_t budget_ns, int32_t* steps_done, double* t_end);
+
 /* The reference-facing batched integrate: host R (total_beads*3), host rng
    (n_chains*3), host status (n_chains). Runs every chain over its own
    bdcu_sim [time_start, time_end] with a cold spectral cache, as

@@ -139,3 +139,38 @@ CASES = [
     "cfg4_fene_b100_cheb", "cfg5_ff_bend_sdk_cheb", "cfg5_ff_bend_sdk_cholesky", "ilc_timeflow_external",
     "wlcbounded_free", "fraenkel_lj_equil_nocom", "n2_dumbbell_hi", "n3_bend_hi_chol",
 ]
+
+
+def build_large_case(name, N, n_steps=2, seed=0):
+    """Full-size chains of the large-chain configurations (a few steps, for
+    parity at sizes where D is held in global memory):
+
+    cfg5_*: FENE-Fraenkel springs (sigma=1, dQ=0.1 -> sqrtb 0.1), bending
+    stiffness 5, SDK excluded volume (d*=1, uniform phi=0.5, cutoff 1.5),
+    h*=0.3 HI by Chebyshev or Cholesky, shear 0.1, dt=1e-4, R0 from
+    fene_fraenkel_bending_chain(N, 1.0, 0.1, 5.0, seed).
+    cfg3_wlc_lj: Marko-Siggia WLC with Q0=20, LJ EV (0.3, 1.0, cutoff 2.5),
+    h*=0.2 Chebyshev, uniaxial 0.5, dt=5e-4, gaussian_chain(N, seed).
+    """
+    p = PhysParams()
+    if name in ("cfg5_cheb", "cfg5_cholesky"):
+        p.spring.type, p.spring.sqrtb, p.spring.natural_length = Spring.FENEFraenkel, 0.1, 1.0
+        p.bend.type, p.bend.stiffness = Bending.OneMinusCosTheta, 5.0
+        p.ev.type, p.ev.dstar, p.ev.max_cutoff = EV.SDK, 1.0, 1.5
+        p.ev.phi = [0.5] * (N * N)
+        p.hstar = 0.3
+        p.hi_method = DelSMethod.Cholesky if name == "cfg5_cholesky" else DelSMethod.Chebyshev
+        p.flow = _shear(0.1)
+        R0 = initial.fene_fraenkel_bending_chain(N, 1.0, 0.1, 5.0, seed=seed)
+        sim = _sim(1e-4, n_steps)
+    elif name == "cfg3_wlc_lj":
+        p.spring.type, p.spring.sqrtb = Spring.WLC, 20.0
+        p.hstar, p.hi_method = 0.2, DelSMethod.Chebyshev
+        p.ev.type, p.ev.zstar, p.ev.dstar, p.ev.max_cutoff = EV.LJ, 0.3, 1.0, 2.5
+        p.flow = _uniaxial(0.5)
+        R0 = initial.gaussian_chain(N, seed=seed)
+        sim = _sim(5e-4, n_steps)
+    else:
+        raise KeyError(name)
+    p.number_of_beads = len(R0)
+    return np.ascontiguousarray(R0, dtype=np.float64), p, sim, seed + 1

@@ -110,3 +110,18 @@ def test_stream_replay_reports_latency_percentiles():
     assert st["jobs_completed"] == 5 and st["jobs_rejected"] == 0
     assert st["chain_steps"] == sum(j.n_traj * j.n_steps for j in jobs)
     assert 0 < st["p50_latency_s"] <= st["p99_latency_s"]
+
+
+def test_sjf_admits_the_smallest_queued_job_first():
+    # room for two chains: A runs, B (more work) and C (less) wait; when A
+    # is done the "sjf" policy admits C first, "fifo" admits B first
+    for policy, first in (("sjf", 2), ("fifo", 1)):
+        srv = _server("mixed", policy=policy, max_active_chains=2)
+        a = srv.submit(_job(40, 2, 200, 1))
+        srv.step()
+        b = srv.submit(_job(40, 2, 300, 2))
+        c = srv.submit(_job(12, 2, 100, 3))
+        srv.run_until_idle()
+        assert all(j.state == "done" for j in (a, b, c))
+        order = sorted((b, c), key=lambda j: j.t_admit)
+        assert order[0] is (c if first == 2 else b), policy
