@@ -186,8 +186,17 @@ def pack_batch(phys_list, sim_list, n_beads_list):
     arena = _Arena()
     phys_arr = (BdcuPhys * max(n, 1))()
     sim_arr = (BdcuSim * max(n, 1))()
+    # chains that share a PhysParams object (and a bead count) share its
+    # record and its arena tables (flow and force samples, the N x N SDK phi)
+    first = {}
     for i in range(n):
-        _fill_phys(phys_arr[i], phys_list[i], n_beads_list[i], arena)
+        key = (id(phys_list[i]), int(n_beads_list[i]))
+        j = first.get(key)
+        if j is None:
+            _fill_phys(phys_arr[i], phys_list[i], n_beads_list[i], arena)
+            first[key] = i
+        else:
+            phys_arr[i] = phys_arr[j]
         _fill_sim(sim_arr[i], sim_list[i])
     return phys_arr, sim_arr, arena.array()
 

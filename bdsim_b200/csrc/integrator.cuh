@@ -25,14 +25,17 @@ namespace bdcu {
 
 constexpr int kSlots = 16;     // n-vectors in shared memory
 constexpr int kCoefCap = 504;  // >= kMaxCheb + 1
-// Blocked Cholesky (3N >= kBlockedCholMin): panels of up to kCholMaxPanel
-// columns, trailing update in kCholTile x kCholTile tiles whose panel rows are
-// staged in shared memory with row stride kCholTileStride (padded against
-// bank conflicts), in vector slots kCholFirstSlot.. (free while D is factored).
+// Blocked Cholesky (3N >= kBlockedCholMin): column blocks of up to
+// kCholMaxBlock columns, each factored as sub-panels of up to kCholMaxPanel
+// columns (rows solved with the sub-panel in registers); trailing updates in
+// kCholTile x kCholTile tiles whose panel rows are staged in shared memory
+// with row stride kCholTileStride (padded against bank conflicts), in vector
+// slots kCholFirstSlot.. (free while D is factored).
 constexpr int kBlockedCholMin = 300;
 constexpr int kCholTile = 64;
 constexpr int kCholTileStride = kCholTile + 8;
-constexpr int kCholMaxPanel = 32;  // panel rows are solved with the panel in registers
+constexpr int kCholMaxPanel = 32;
+constexpr int kCholMaxBlock = 64;
 constexpr int kCholFirstSlot = 7;
 
 // Block-shared control state.
@@ -375,61 +378,72 @@ struct Block {
         return true;
     }
 
-    // Panel width of the blocked factorisation (0: unblocked): up to
-    // kCholMaxPanel columns, a multiple of 8, such that two staged tiles of
+    // Column-block width of the blocked factorisation (0: unblocked): up to
+    // kCholMaxBlock columns, a multiple of 8, such that two staged tiles of
     // panel rows fit the staging area.
     __device__ int chol_panel_width() const {
         if (n < kBlockedCholMin || stage == nullptr) return 0;
         int64_t nb = stage_cap / (2 * kCholTileStride);
-        nb = nb > kCholMaxPanel ? kCholMaxPanel : nb;
+        nb = nb > kCholMaxBlock ? kCholMaxBlock : nb;
         nb &= ~7;
         return nb >= 8 ? (int)nb : 0;
     }
 
-    // Blocked right-looking Cholesky. For each panel of nb columns [kb, ke):
-    // (1) the panel's diagonal block is factored in shared memory column by
-    //     column (pivot, scale, then the block's remaining columns updated);
-    //     each row below it is then solved by one thread, its nb panel
-    //     entries in registers: L(i,j) = (A(i,j) - sum_{k<j} L(i,k) L(j,k)) /
-    //     L(j,j) for j = kb, kb+1, ... in order;
-    // (2) the trailing lower triangle [ke, n)^2 is updated by the panel,
+    // Blocked right-looking Cholesky. For each column block [kb, ke) of up to
+    // nb columns:
+    // (1) the block is factored as sub-panels [p0, p1) of up to kCholMaxPanel
+    //     columns: the sub-panel's columns (rows >= p0) first receive the
+    //     products of the block's earlier columns k in [kb, p0) (trailing
+    //     update restricted to columns [p0, p1)); then its diagonal block is
+    //     factored in shared memory column by column (pivot, scale, update
+    //     of the remaining columns) and each row below it is solved by one
+    //     thread, its sub-panel entries in registers: L(i,j) = (A(i,j) -
+    //     sum_{k<j} L(i,k) L(j,k)) / L(j,j) for j = p0, p0+1, ... in order;
+    // (2) the trailing lower triangle [ke, n)^2 is updated by the block,
     //     C(i,j) -= sum_{k in [kb,ke)} L(i,k) L(j,k), tile by tile, with the
     //     tile's panel rows staged in shared memory.
     // Every element still receives its products in k order before its
     // division, so the plain form keeps the reference's rounding sequence
-    // (trailing update one rounded product and one rounded subtraction per
-    // k); the mixed form's trailing update runs on the FP64 tensor cores
+    // (trailing updates one rounded product and one rounded subtraction per
+    // k); the mixed form's trailing updates run on the FP64 tensor cores
     // (mma.m8n8k4, products accumulated in the tensor core's own order).
     __device__ bool cholesky_blocked(int nb) {
-        double* L = Lt;
-        double* As = stage;                          // As[k*TS + r] = L(i0 + r, kb + k)
-        double* Bs = stage + (int64_t)nb * kCholTileStride;  // Bs[k*TS + c] = L(j0 + c, kb + k)
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
         for (int kb = 0; kb < n; kb += nb) {
             const int ke = kb + nb < n ? kb + nb : n;
-            if (!chol_panel(kb, ke)) return false;
-            if (ke >= n) break;
-            const int kk = ke - kb;
-            const int mt = (n - ke + kCholTile - 1) / kCholTile;
-            for (int tt = 0; tt < mt * (mt + 1) / 2; ++tt) {
-                int ti = (int)((sqrt(8.0 * tt + 1.0) - 1.0) * 0.5);
-                while (ti * (ti + 1) / 2 > tt) --ti;
-                while ((ti + 1) * (ti + 2) / 2 <= tt) ++ti;
-                const int tj = tt - ti * (ti + 1) / 2;  // tile (ti, tj), tj <= ti
-                const int i0 = ke + ti * kCholTile, j0 = ke + tj * kCholTile;
-                for (int e = threadIdx.x; e < nb * kCholTile; e += blockDim.x) {
-                    const int k = e / kCholTile, r = e % kCholTile;
-                    const bool kin = k < kk;
-                    As[k * kCholTileStride + r] = (kin && i0 + r < n) ? L[(int64_t)(kb + k) * n + i0 + r] : 0.0;
-                    Bs[k * kCholTileStride + r] = (kin && j0 + r < n) ? L[(int64_t)(kb + k) * n + j0 + r] : 0.0;
-                }
-                __syncthreads();
-                if constexpr (!kMixed) chol_tile_simt(As, Bs, i0, j0, kk);
-                else chol_tile_dmma(As, Bs, i0, j0, (kk + 3) & ~3, warp, lane, nwarps);
-                __syncthreads();
+            for (int p0 = kb; p0 < ke; p0 += kCholMaxPanel) {
+                const int p1 = p0 + kCholMaxPanel < ke ? p0 + kCholMaxPanel : ke;
+                if (p0 > kb) chol_update(kb, p0, p0, p0, p1);
+                if (!chol_panel(p0, p1)) return false;
             }
+            if (ke >= n) break;
+            chol_update(kb, ke, ke, ke, n);
         }
         return true;
+    }
+
+    // C(i,j) -= sum_{k in [k0,k1)} L(i,k) L(j,k) (k in order) for columns j in
+    // [c0, c1) and rows i in [r0, n), i >= j, in kCholTile^2 tiles.
+    __device__ void chol_update(int k0, int k1, int r0, int c0, int c1) {
+        double* L = Lt;
+        const int kk = k1 - k0, kk4 = (kk + 3) & ~3;  // staged rows k >= kk are zero
+        double* As = stage;                                   // As[k*TS + r] = L(i0 + r, k0 + k)
+        double* Bs = stage + (int64_t)kk4 * kCholTileStride;  // Bs[k*TS + c] = L(j0 + c, k0 + k)
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        const int nti = (n - r0 + kCholTile - 1) / kCholTile, ntj = (c1 - c0 + kCholTile - 1) / kCholTile;
+        for (int t = 0; t < nti * ntj; ++t) {
+            const int i0 = r0 + (t / ntj) * kCholTile, j0 = c0 + (t % ntj) * kCholTile;
+            if (i0 + kCholTile - 1 < j0) continue;  // all above the diagonal
+            for (int e = threadIdx.x; e < kk4 * kCholTile; e += blockDim.x) {
+                const int k = e / kCholTile, r = e % kCholTile;
+                const bool kin = k < kk;
+                As[k * kCholTileStride + r] = (kin && i0 + r < n) ? L[(int64_t)(k0 + k) * n + i0 + r] : 0.0;
+                Bs[k * kCholTileStride + r] = (kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * n + j0 + r] : 0.0;
+            }
+            __syncthreads();
+            if constexpr (!kMixed) chol_tile_simt(As, Bs, i0, j0, c1, kk);
+            else chol_tile_dmma(As, Bs, i0, j0, c1, kk4, warp, lane, nwarps);
+            __syncthreads();
+        }
     }
 
     // Panel [kb, ke) of the blocked factorisation (step 1 above). The
@@ -489,7 +503,7 @@ struct Block {
     // Trailing-update tile, FP64 CUDA cores: 4x4 elements per thread, each
     // element c = c - a_k * b_k for k = 0, 1, ... (no contraction: the plain
     // form is compiled without FMA).
-    __device__ void chol_tile_simt(const double* As, const double* Bs, int i0, int j0, int kk) {
+    __device__ void chol_tile_simt(const double* As, const double* Bs, int i0, int j0, int jend, int kk) {
         double* L = Lt;
         constexpr int Q = kCholTile / 4;
         for (int mtl = threadIdx.x; mtl < Q * Q; mtl += blockDim.x) {
@@ -501,7 +515,7 @@ struct Block {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     const int i = i0 + r0 + u, j = j0 + c0 + v;
-                    c[u][v] = (i < n && j < n && i >= j) ? L[(int64_t)j * n + i] : 0.0;
+                    c[u][v] = (i < n && j < jend && i >= j) ? L[(int64_t)j * n + i] : 0.0;
                 }
             for (int k = 0; k < kk; ++k) {
                 const double2 a01 = *reinterpret_cast<const double2*>(As + k * kCholTileStride + r0);
@@ -519,38 +533,58 @@ struct Block {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     const int i = i0 + r0 + u, j = j0 + c0 + v;
-                    if (i < n && j < n && i >= j) L[(int64_t)j * n + i] = c[u][v];
+                    if (i < n && j < jend && i >= j) L[(int64_t)j * n + i] = c[u][v];
                 }
         }
     }
 
     // Trailing-update tile on the FP64 tensor cores: the tile is 8x8 blocks
-    // of 8x8; warp w takes blocks w, w + nwarps, ...; each block is
+    // of 8x8; warp w takes blocks w, w + nwarps, ..., four at a time (their C
+    // fragments loaded together before the k loop); each block is
     // C += (-A) B over k in steps of 4 with mma.sync.m8n8k4.f64 (A 8x4 row:
     // lane holds A[lane/4][lane%4]; B 4x8 col: lane holds B[lane%4][lane/4];
     // C 8x8: lane holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]).
-    // kk4: the panel width rounded up to 4 (the staged rows are zero beyond).
-    __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int kk4, int warp, int lane,
-                                   int nwarps) {
+    // jend: columns from jend on are left alone. kk4: the panel width rounded
+    // up to 4 (the staged rows are zero beyond).
+    __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int jend, int kk4, int warp,
+                                   int lane, int nwarps) {
         double* L = Lt;
         constexpr int B8 = kCholTile / 8;
         const int g = lane >> 2, q = lane & 3;
-        for (int blk = warp; blk < B8 * B8; blk += nwarps) {
-            const int tr = (blk % B8) * 8, tc = (blk / B8) * 8;
-            if (i0 + tr + 7 < j0 + tc) continue;  // all above the diagonal
-            const int i = i0 + tr + g, ja = j0 + tc + 2 * q, jb = ja + 1;
-            const bool oka = i < n && ja < n && i >= ja, okb = i < n && jb < n && i >= jb;
-            double c0 = oka ? L[(int64_t)ja * n + i] : 0.0;
-            double c1 = okb ? L[(int64_t)jb * n + i] : 0.0;
-            for (int k = 0; k < kk4; k += 4) {
-                const double av = -As[(k + q) * kCholTileStride + tr + g];
-                const double bv = Bs[(k + q) * kCholTileStride + tc + g];
-                asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                             : "+d"(c0), "+d"(c1)
-                             : "d"(av), "d"(bv));
+        for (int b0 = warp; b0 < B8 * B8; b0 += 4 * nwarps) {
+            double c[4][2];
+            int tr[4], tc[4];
+            bool act[4], oka[4], okb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int blk = b0 + u * nwarps;
+                tr[u] = (blk % B8) * 8;
+                tc[u] = (blk / B8) * 8;
+                act[u] = blk < B8 * B8 && !(i0 + tr[u] + 7 < j0 + tc[u]);  // warp-uniform
+                const int i = i0 + tr[u] + g, ja = j0 + tc[u] + 2 * q, jb = ja + 1;
+                oka[u] = act[u] && i < n && ja < jend && i >= ja;
+                okb[u] = act[u] && i < n && jb < jend && i >= jb;
+                c[u][0] = oka[u] ? L[(int64_t)ja * n + i] : 0.0;
+                c[u][1] = okb[u] ? L[(int64_t)jb * n + i] : 0.0;
             }
-            if (oka) L[(int64_t)ja * n + i] = c0;
-            if (okb) L[(int64_t)jb * n + i] = c1;
+            for (int k = 0; k < kk4; k += 4) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (act[u]) {
+                        const double av = -As[(k + q) * kCholTileStride + tr[u] + g];
+                        const double bv = Bs[(k + q) * kCholTileStride + tc[u] + g];
+                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                     : "+d"(c[u][0]), "+d"(c[u][1])
+                                     : "d"(av), "d"(bv));
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = i0 + tr[u] + g, ja = j0 + tc[u] + 2 * q;
+                if (oka[u]) L[(int64_t)ja * n + i] = c[u][0];
+                if (okb[u]) L[(int64_t)(ja + 1) * n + i] = c[u][1];
+            }
         }
     }
 

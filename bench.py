@@ -264,6 +264,72 @@ def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed
     return st
 
 
+OTHER_WORKLOADS = {
+    "cfg3": ("uneven batch: 8192 chains, N ~ U{20..200} (seeded), Marko-Siggia WLC with Q0 ~ U[10,30], h*=0.2 "
+             "Chebyshev, uniaxial extension 0.5, LJ EV (0.3, 1.0, cut 2.5), dt=5e-4, FP64 connector solve; "
+             "block shapes autotuned per N bucket", 8192, 20),
+    "cfg5-cheb": ("large stiff chains: 1024 x N=500 FENE-Fraenkel (sigma 1, dQ 0.1) + bending 5 + SDK EV (d*=1, "
+                  "uniform phi 0.5), h*=0.3 Chebyshev (FP64 Lanczos bounds), shear 0.1, dt=1e-4", 1024, 5),
+    "cfg5-chol": ("large stiff chains: 1024 x N=500 as cfg5-cheb with the Cholesky square root (blocked; FP64 "
+                  "tensor-core trailing updates in the mixed form)", 1024, 1),
+}
+
+
+def other_workload(torch, name, steps, warmup, forms, n_chains=None):
+    """One JSON line for a non-headline configuration: chain-steps/s of each
+    form over `steps` timed chunks (CUDA events on the launch stream, L2
+    flushed between chunks)."""
+    import bdsim_b200 as B
+    from bdsim_b200 import workloads
+    from bdsim_b200._abi import CACHE_PERSIST
+    from bdsim_b200.params import DelSMethod
+    desc, n, chunk = OTHER_WORKLOADS[name]
+    n = n_chains or n
+    if name == "cfg3":
+        phys, sims, Rs, seeds = workloads.uneven_wlc(n, seed=0)
+    else:
+        method = DelSMethod.Cholesky if name == "cfg5-chol" else DelSMethod.Chebyshev
+        phys, sims, Rs, seeds = workloads.stiff_large(n, 0, 500, method)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = {}
+    for form in forms:
+        with torch.cuda.stream(stream):
+            ens = B.Ensemble(phys, sims, Rs, [(1, -1, s) for s in seeds], form=form)
+            tuned = ens.autotune() if name == "cfg3" else None
+            dt = np.array([s.dt for s in sims])
+            t = np.array([s.time_start for s in sims])
+            for _ in range(warmup):
+                ens.advance(t, chunk, CACHE_PERSIST)
+                t = t + chunk * dt
+            stream.synchronize()
+            c0 = ens.counter_totals()
+            ms = []
+            for _ in range(steps):
+                flush_l2(torch, flush)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ens.advance(t, chunk, CACHE_PERSIST)
+                e1.record(stream)
+                t = t + chunk * dt
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            c1 = ens.counter_totals()
+            out[form] = {"value": n * chunk * steps / (sum(ms) * 1e-3), "ms_per_chunk": float(np.mean(ms)),
+                         "failed": int(ens.failed().sum()), "plan": ens.plan(), "tuned": tuned,
+                         "counters_per_step": {k: (c1[k] - c0[k]) / max(c1["steps"] - c0["steps"], 1) for k in c1}}
+        del ens
+    line = {"metric": "chain-steps/sec", "workload": name, "value": out.get("mixed", out[forms[0]])["value"],
+            "unit": "chain-steps/s", "n_gpus": 1, "steps": steps, "warmup": warmup, "chunk_steps": chunk,
+            "higher_is_better": True, "data": "synthetic", "config": {"workload": desc, "n_chains": n},
+            "forms": out}
+    if "mixed" in out and "plain" in out:
+        line["mixed_over_plain"] = out["mixed"]["value"] / out["plain"]["value"]
+    print(json.dumps(line))
+    return 0
+
+
 def cpu_reference(seconds_target=15.0, threads=None):
     """The reference C++ step (oracle/_ref, compiled from the reference
     sources; the C restatement when that library is absent) on the host
@@ -318,8 +384,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer e2e leg (profiling runs)")
-    ap.add_argument("--chains", type=int, default=N_CHAINS, help="chains per GPU (profiling runs use fewer)")
+    ap.add_argument("--chains", type=int, default=None,
+                    help="chains per GPU (default: the workload's; profiling runs use fewer)")
     ap.add_argument("--forms", default="plain,mixed", help="integrator forms to time")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2"] + sorted(OTHER_WORKLOADS),
+                    help="cfg2 (default): the headline line; others print their own line")
     ap.add_argument("--serving-seconds", type=float, default=60.0,
                     help="length of the serving replay (0: skip it)")
     args = ap.parse_args()
@@ -352,13 +421,18 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.workload != "cfg2":
+        if rank != 0:
+            return 0
+        return other_workload(torch, args.workload, args.steps, args.warmup,
+                              [f for f in args.forms.split(",") if f], args.chains)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     phys, sim = make_phys()
-    n_chains = args.chains
+    n_chains = args.chains or N_CHAINS
     Rs = make_chains(rank * n_chains, n_chains)
     stream = torch.cuda.Stream()
 

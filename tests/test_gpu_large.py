@@ -27,7 +27,8 @@ def rel(a, b):
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(1.0, float(np.max(np.abs(b)))))
 
 
-CASES = [("cfg5_cholesky", 500), ("cfg5_cholesky", 150), ("cfg5_cholesky", 100), ("cfg5_cheb", 500),
+CASES = [("cfg5_cholesky", 500), ("cfg5_cholesky", 250), ("cfg5_cholesky", 150), ("cfg5_cholesky", 100),
+         ("cfg5_cheb", 500),
          ("cfg3_wlc_lj", 200)]
 
 
