@@ -432,8 +432,13 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     phys, sim = make_phys()
+    from bdsim_b200.sharding import reduce_max, shard_bounds
     n_chains = args.chains or N_CHAINS
-    Rs = make_chains(rank * n_chains, n_chains)
+    # weak scaling: world shards of n_chains each, the global chain index is
+    # the seed, so the shards together are the single-GPU ensemble of
+    # world * n_chains chains
+    first, _ = shard_bounds(np.ones(world * n_chains), world)[rank]
+    Rs = make_chains(first, n_chains)
     stream = torch.cuda.Stream()
 
     def barrier():
@@ -449,20 +454,14 @@ def main():
         sampler = ClockSampler(local) if form == "mixed" else None
         if sampler:
             sampler.start()
-        r = run_form(torch, form, Rs, phys, sim, args.steps, args.warmup, rank * n_chains, stream)
+        r = run_form(torch, form, Rs, phys, sim, args.steps, args.warmup, first, stream)
         if sampler:
             clocks = sampler.stop()
         barrier()
-        tot = sum(r["ms"])
-        if dist is not None:
-            t = torch.tensor([tot], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot = float(t.item())
-        r["total_ms"] = tot
+        r["total_ms"] = reduce_max(sum(r["ms"]), dist, device="cuda")
         results[form] = r
 
-    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), 1, rank * n_chains,
-                                           "mixed")
+    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), 1, first, "mixed")
     serving = None
     if args.serving_seconds > 0 and set(forms) == {"plain", "mixed"}:
         serving = run_serving(torch, args.serving_seconds, seed=rank)
