@@ -248,6 +248,8 @@ def load_library():
     lib.bdcu_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
     lib.bdcu_destroy.argtypes = [vp]
     lib.bdcu_set_stream.argtypes = [vp, vp]
+    lib.bdcu_set_bounds_refresh.argtypes = [vp, ctypes.c_int]
+    lib.bdcu_observables.argtypes = [vp, vp, vp, vp]
     lib.bdcu_last_error.argtypes = [vp]
     lib.bdcu_last_error.restype = ctypes.c_char_p
     lib.bdcu_set_chains.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim),

@@ -26,6 +26,8 @@ cudaError_t occupancy_mixed_team(int team_warps, size_t smem, int* per_sm);
 cudaError_t launch_forces(const DevChain* chains, int n_chains, int n_max, const double* arena, const double* R,
                           double t, int which, double* F, cudaStream_t s);
 cudaError_t launch_ran1(int n_chains, int32_t* rng, int n_per, double* out, cudaStream_t s);
+cudaError_t launch_observables(const DevChain* chains, int n_chains, const double* R, const double* F, double* out,
+                               cudaStream_t s);
 cudaError_t launch_scatter_records(DevChain* dst, const DevChain* src, const int32_t* slots, int count,
                                    cudaStream_t s);
 }  // namespace bdcu
@@ -483,6 +485,7 @@ int launch_bucket(bdcu_ctx* ctx, int form, const Bucket& b, const State& st, int
     a.budget_ns = st.budget_ns;
     a.steps_done = st.steps_done;
     a.t_end = st.t_end;
+    a.bounds_every = form == BDCU_FORM_MIXED_FP32 ? ctx->bounds_every : 1;
     cudaError_t e;
     if (b.kernel == BDCU_KERNEL_TEAM)
         e = launch_mixed_team(b.team_warps, a, b.grid, b.smem, s);
@@ -664,6 +667,13 @@ int bdcu_run_slice(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache, int32_
     st.steps_done = steps_done;
     st.t_end = t_end;
     return run_plan(ctx, form, st, cache_mode);
+}
+
+int bdcu_set_bounds_refresh(bdcu_ctx* ctx, int every_steps) {
+    if (!ctx) return BDCU_E_ARG;
+    if (every_steps < 1 || every_steps > 1000000) return fail(ctx, BDCU_E_ARG, "every_steps must be in [1, 1e6]");
+    ctx->bounds_every = every_steps;
+    return BDCU_OK;
 }
 
 int bdcu_describe_plan(bdcu_ctx* ctx, int form, bdcu_bucket_info* out, int cap, int* n_out) {
@@ -987,6 +997,16 @@ int bdcu_forces(bdcu_ctx* ctx, const double* R, double t, int which, double* F) 
 
 int bdcu_total_force(bdcu_ctx* ctx, const double* R, double* F) {
     return bdcu_forces(ctx, R, 0.0, BDCU_F_SPRING | BDCU_F_EV | BDCU_F_BEND, F);
+}
+
+int bdcu_observables(bdcu_ctx* ctx, const double* R, const double* F, double* out) {
+    if (!ctx) return BDCU_E_ARG;
+    if (ctx->n_chains < 1) return fail(ctx, BDCU_E_STATE, "bdcu_observables before bdcu_set_chains");
+    if (!R || !F || !out) return fail(ctx, BDCU_E_ARG, "null device pointer");
+    CK(cudaSetDevice(ctx->device));
+    cudaError_t e = launch_observables(ctx->chains_d, ctx->n_chains, R, F, out, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "observables kernel launch");
+    return BDCU_OK;
 }
 
 int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double* out) {

@@ -90,6 +90,51 @@ cudaError_t launch_forces(const DevChain* chains, int n_chains, int n_max, const
     return cudaGetLastError();
 }
 
+// Per-chain observables of a configuration (python/bdsim/properties.py:13-41):
+// out[c*10 + 0] = Rg^2 = trace of the gyration tensor, out[c*10 + 1 + 3i + j]
+// = Kramers stress tau_ij = sum_mu (R_mu - R_c)_i F_mu,j. One warp per chain,
+// sums over beads in a warp butterfly (not the host's order: last-bit
+// differences from numpy).
+__global__ void observables_kernel(const DevChain* __restrict__ chains, int n_chains, const double* __restrict__ R,
+                                   const double* __restrict__ F, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_chains; c += nw) {
+        const int N = chains[c].N;
+        const double* r = R + 3 * chains[c].bead_off;
+        const double* f = F + 3 * chains[c].bead_off;
+        double s[10];
+        for (int d = 0; d < 3; ++d) s[d] = 0.0;
+        for (int m = lane; m < N; m += 32)
+            for (int d = 0; d < 3; ++d) s[d] += r[3 * m + d];
+        for (int d = 0; d < 3; ++d) {
+            for (int o = 16; o > 0; o >>= 1) s[d] += __shfl_xor_sync(0xffffffffu, s[d], o);
+        }
+        const double inv = N > 0 ? 1.0 / N : 0.0;
+        const double cx = s[0] * inv, cy = s[1] * inv, cz = s[2] * inv;
+        for (int k = 0; k < 10; ++k) s[k] = 0.0;
+        for (int m = lane; m < N; m += 32) {
+            const double x[3] = {r[3 * m] - cx, r[3 * m + 1] - cy, r[3 * m + 2] - cz};
+            s[0] += x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) s[1 + 3 * i + j] += x[i] * f[3 * m + j];
+        }
+        for (int k = 0; k < 10; ++k)
+            for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+        if (lane == 0) {
+            out[10 * (int64_t)c] = s[0] * inv;
+            for (int k = 1; k < 10; ++k) out[10 * (int64_t)c + k] = s[k];
+        }
+    }
+}
+
+cudaError_t launch_observables(const DevChain* chains, int n_chains, const double* R, const double* F, double* out,
+                               cudaStream_t s) {
+    const int warps = n_chains < 148 * 64 ? n_chains : 148 * 64;
+    observables_kernel<<<(warps + 7) / 8, 256, 0, s>>>(chains, n_chains, R, F, out);
+    return cudaGetLastError();
+}
+
 // ran_1 with lazy seeding (Rng::maybe_init, src/rng.cpp:31-39), one thread per stream.
 __global__ void ran1_kernel(int n_chains, int32_t* rng, int n_per, double* out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;

@@ -82,6 +82,10 @@ struct RunArgs {
     int64_t budget_ns;
     int32_t* steps_done;
     double* t_end;
+    // FP32-mixed team kernel: spectral bounds recomputed every bounds_every
+    // steps (1: every step, the reference) and whenever a step's Chebyshev
+    // check fails on the kept ones
+    int32_t bounds_every;
 };
 
 // Nanoseconds of the GPU's global timer.

@@ -82,6 +82,7 @@ struct bdcu_ctx {
     int seed_len = 0;
     int32_t* work_d = nullptr;  // one queue counter per bucket
     int sm_count = 148;
+    int bounds_every = 1;  // bdcu_set_bounds_refresh
     size_t max_smem = 0;
     // the chains bdcu_run advances: all records (sel_all) or a list (bdcu_select)
     int sel_all = 1;

@@ -947,13 +947,15 @@ struct TeamChain {
     // The step's three mutually independent products against D(R) run in
     // one pass first: D v0 (the Lanczos start vector), D X0 (the noise, for
     // the Chebyshev series) and D A (A = Fs + Fe, the predictor's force).
+    // fuse: also form DX0 = D X0 and DA = D A in the start vector's pass;
+    // otherwise the caller has them and the Lanczos forms D v0 itself.
     __device__ void bounds(double* cache, int& cache_valid, double& lmin, double& lmax, const float (&X0)[2][3],
-                           const float (&A)[2][3], float (&DX0)[2][3], float (&DA)[2][3]) {
+                           const float (&A)[2][3], float (&DX0)[2][3], float (&DA)[2][3], bool fuse = true) {
         double vmin[2][3], vmax[2][3], rmin, rmax;
         const bool can_warm = cache_valid != 0;
         double v0[2][3], dv0[2][3];
         start_vector(can_warm, cache, v0);
-        {
+        if (fuse) {
             float x3[3][2][3], y3[3][2][3];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
@@ -974,7 +976,7 @@ struct TeamChain {
                 }
         }
         const int steps =
-            lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, v0, dv0, true, vmin, vmax, rmin, rmax);
+            lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, v0, dv0, fuse, vmin, vmax, rmin, rmax);
         if (can_warm && steps < 4) {
             start_vector(false, cache, v0);
             lanczos(kLanczosCold, false, v0, dv0, false, vmin, vmax, rmin, rmax);
@@ -1009,9 +1011,11 @@ struct TeamChain {
 
     // ---- Chebyshev square root, FP32 recurrence (src/hydrodynamics.cpp:267-337)
     // Returns the FD error; out = approx D^{1/2} x0.
-    // Dx0 = D x0 (computed by the caller).
+    // Dx0 = D x0 (computed by the caller). grow: the FD growth loop of the
+    // reference; without it a failed check returns at once (bounds kept from
+    // an earlier step are refreshed first).
     __device__ double chebyshev(const float (&x0)[2][3], const float (&Dx0)[2][3], double lmin, double lmax,
-                                float (&out)[2][3]) {
+                                float (&out)[2][3], bool grow = true) {
         const double x0Dx0 = dotf(x0, Dx0);
         double Lr = sqrt(lmax / lmin) * ch.mult + 0.5;
         int L = !(Lr < 2.0e9) ? kMaxCheb : (int)Lr + 1;
@@ -1067,7 +1071,7 @@ struct TeamChain {
             const double rr = dotf(out, out);
             fd = fabs(rr - x0Dx0) / x0Dx0;
             sync();
-            if (fd <= ch.fd_tol || L >= kMaxCheb) break;
+            if (fd <= ch.fd_tol || L >= kMaxCheb || !grow) break;
             const int grow = L / 4 > 1 ? L / 4 : 1;
             L = (L + grow) > kMaxCheb ? kMaxCheb : L + grow;
         }
@@ -1221,6 +1225,10 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
         const double dt = ch.dt;
         const double sqrt2inv = 1.0 / sqrt(2.0);
         const double sqrt_dt = sqrt(dt);
+        // spectral bounds kept between refreshes (a launch starts with a refresh)
+        const int bounds_every = a.bounds_every > 1 ? a.bounds_every : 1;
+        int since_bounds = bounds_every;
+        double lmin = 0.0, lmax = 0.0;
         int step = 0;
         for (; step < nsteps; ++step) {
             // time slice: no new step past the budget (thread 0 decides for the team)
@@ -1251,14 +1259,42 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
 #pragma unroll
                     for (int d = 0; d < 3; ++d) dW[q][d] = (float)(sqrt_dt * X0[q][d]);
             } else {
-                double lmin, lmax;
                 float bx[2][3], DX0[2][3];
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) A[q][d] = Fs[q][d] + Fe[q][d];
-                W.bounds(gcache, cache_valid, lmin, lmax, X0, A, DX0, DF);
-                const double fd = W.chebyshev(X0, DX0, lmin, lmax, bx);
+                double fd;
+                if (since_bounds >= bounds_every) {
+                    W.bounds(gcache, cache_valid, lmin, lmax, X0, A, DX0, DF);
+                    since_bounds = 0;
+                    fd = W.chebyshev(X0, DX0, lmin, lmax, bx);
+                } else {
+                    // bounds kept from an earlier step: the two products in one pass
+                    float x2[2][2][3], y2[2][2][3];
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            x2[0][q][d] = X0[q][d];
+                            x2[1][q][d] = A[q][d];
+                        }
+                    W.template applyK<2>(x2, y2);
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            DX0[q][d] = y2[0][q][d];
+                            DF[q][d] = y2[1][q][d];
+                        }
+                    fd = W.chebyshev(X0, DX0, lmin, lmax, bx, false);
+                    if (!(fd <= ch.fd_tol)) {  // the kept bounds no longer hold: refresh and redo
+                        W.bounds(gcache, cache_valid, lmin, lmax, X0, A, DX0, DF, false);
+                        since_bounds = 0;
+                        fd = W.chebyshev(X0, DX0, lmin, lmax, bx);
+                    }
+                }
+                ++since_bounds;
                 if (!(fd <= ch.fd_tol)) {
                     W.status |= BDCU_ST_CHEB_FALLBACK;
                     W.cnt[C_FALLBACK] += 1;

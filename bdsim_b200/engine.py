@@ -75,6 +75,11 @@ class Context:
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         self._ck(self.lib.bdcu_set_stream(self.h, ctypes.c_void_p(s.cuda_stream)), "bdcu_set_stream")
 
+    def set_bounds_refresh(self, every_steps: int):
+        """FP32-mixed form: recompute the spectral bounds every `every_steps`
+        steps (and on a failed Chebyshev check); 1 is the reference's policy."""
+        self._ck(self.lib.bdcu_set_bounds_refresh(self.h, int(every_steps)), "bdcu_set_bounds_refresh")
+
     def set_chains(self, phys_list, sim_list, n_beads_list):
         prec, srec, arena = _abi.pack_batch(phys_list, sim_list, n_beads_list)
         self._arena = arena
@@ -281,6 +286,16 @@ class Ensemble:
         self.ctx.total_force(self.R, F)
         Fh = F.cpu().numpy()
         return [Fh[self.offsets[i]:self.offsets[i + 1]].copy() for i in range(self.n)]
+
+    def observables(self):
+        """(n, 10) per chain on the device: [Rg^2, tau_xx, tau_xy, ..., tau_zz]
+        (Kramers stress with the total force, python/bdsim/properties.py)."""
+        torch = self.torch
+        F = torch.empty_like(self.R)
+        self.ctx.total_force(self.R, F)
+        out = torch.empty((self.n, 10), dtype=torch.float64, device=self.dev)
+        self.ctx._ck(self.ctx.lib.bdcu_observables(self.ctx.h, dptr(self.R), dptr(F), dptr(out)), "bdcu_observables")
+        return out.cpu().numpy()
 
     def rng_states(self):
         return [tuple(int(v) for v in row) for row in self.rng.cpu().numpy()]

@@ -173,6 +173,17 @@ int bdcu_create(int device, bdcu_ctx** out);
 int bdcu_destroy(bdcu_ctx* ctx);
 /* Stream for all subsequent work (a cudaStream_t; NULL = legacy default). */
 int bdcu_set_stream(bdcu_ctx* ctx, void* stream);
+
+/* Spectral-bound refresh policy of the FP32-mixed form (no counterpart in the
+   reference, which recomputes the Lanczos bounds every step,
+   src/mobility.cpp:64-67): the team kernel (mixed form, N <= 512) keeps a
+   chain's padded bounds for every_steps steps and recomputes them early when
+   a step's Chebyshev fluctuation-dissipation check fails on the kept bounds
+   (then the reference's growth and Cholesky fallback apply). Every launch
+   starts with a refresh, so with every_steps > 1 a run cut into launches
+   differs from one launch. 1 (the default) is the reference's policy; the
+   plain form always refreshes every step. */
+int bdcu_set_bounds_refresh(bdcu_ctx* ctx, int every_steps);
 /* Message of the last failing call on this context (NUL-terminated). */
 const char* bdcu_last_error(bdcu_ctx* ctx);
 
@@ -239,6 +250,14 @@ int bdcu_total_force(bdcu_ctx* ctx, const double* R, double* F);
    (spring + (EV + bending)) + external, the reference's grouping. */
 enum { BDCU_F_SPRING = 1, BDCU_F_EV = 2, BDCU_F_BEND = 4, BDCU_F_EXTERNAL = 8 };
 int bdcu_forces(bdcu_ctx* ctx, const double* R, double t, int which, double* F);
+
+/* Per-chain observables on the device, for snapshots without a host round
+   trip: radius_of_gyration_sq and kramers_stress (python/bdsim/properties.py:
+   17-19,38-41) of positions R with the forces F (e.g. from bdcu_total_force;
+   device pointers, total_beads*3 each). out: n_chains*10 doubles per record,
+   [Rg^2, tau_xx, tau_xy, tau_xz, tau_yx, tau_yy, tau_yz, tau_zx, tau_zy,
+   tau_zz], tau_ij = sum_mu (R_mu - R_c)_i F_mu,j. */
+int bdcu_observables(bdcu_ctx* ctx, const double* R, const double* F, double* out);
 
 /* Draw n_per_chain uniforms per chain from device RNG states (n_chains*3
    int32, advanced in place) into out (device, n_chains*n_per_chain). */

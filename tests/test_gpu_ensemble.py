@@ -71,3 +71,18 @@ def test_failed_trajectories_are_dropped_and_limited():
     s.dt, s.time_end = 0.01, 0.05
     with pytest.raises(RuntimeError):
         B.run_ensemble(p, s, 3, B.final_state)
+
+
+def test_device_observables_match_numpy():
+    # Rg^2 and the Kramers stress of uneven chains, on the device vs numpy
+    from bdsim_b200 import workloads
+    phys, sims, R0s, seeds = workloads.uneven_wlc(24, seed=3, n_min=2, n_max=90)
+    ens = B.Ensemble(phys, sims, R0s, [(1, -1, s) for s in seeds], form="mixed")
+    ens.advance(0.0, 20)
+    o = ens.observables()
+    Rs, Fs = ens.positions(), ens.total_force()
+    for i, (R, F) in enumerate(zip(Rs, Fs)):
+        X = R - R.mean(axis=0)
+        assert abs(o[i, 0] - np.sum(X * X) / len(R)) <= 1e-12 * max(1.0, o[i, 0])
+        tau = X.T @ F
+        assert np.max(np.abs(o[i, 1:].reshape(3, 3) - tau)) <= 1e-11 * max(1.0, np.max(np.abs(tau)))
