@@ -297,6 +297,27 @@ std::vector<Shape> block_shapes(const bdcu_ctx* ctx, const Bucket& b, int form) 
     return out;
 }
 
+// The heuristic's shape (when none is tuned): the widest block, with D in
+// shared memory unless keeping D in global memory lets more blocks share an
+// SM. D in global stays L2-resident: a D that fits shared memory is at most
+// ~195 KB, ~87 MB over three blocks on each of 148 SMs. Measured at
+// 4096 x N=50 (plain form): D in global with three blocks per SM runs 1.7x
+// the D-in-shared shape's one block per SM.
+Shape default_shape(const Bucket& b, int mixed, const std::vector<Shape>& shapes) {
+    const Shape& first = shapes.front();
+    if (mixed || !first.d_in_smem) return first;
+    for (const Shape& s : shapes) {
+        if (s.block != first.block || s.d_in_smem) continue;
+        int per_d = 0, per_g = 0;
+        const size_t sm_d = (size_t)smem_layout(b.n_max, 1, first.v_cap, 0).total * sizeof(double);
+        const size_t sm_g = (size_t)smem_layout(b.n_max, 0, s.v_cap, 0).total * sizeof(double);
+        if (occupancy_plain(first.block, sm_d, &per_d) != cudaSuccess) return first;
+        if (occupancy_plain(s.block, sm_g, &per_g) != cudaSuccess) return first;
+        return per_g > per_d ? s : first;
+    }
+    return first;
+}
+
 // Fill the launch fields of a bucket for a shape (block kernel) or for the
 // team kernel; 0 when the shape cannot run.
 int fill_launch(bdcu_ctx* ctx, int form, Bucket& b, const Shape* s) {
@@ -399,7 +420,7 @@ int build_plan(bdcu_ctx* ctx, int form) {
         } else {
             const std::vector<Shape> shapes = block_shapes(ctx, b, form);
             if (shapes.empty()) return fail(ctx, BDCU_E_LIMIT, "chain too large for the shared-memory layout");
-            Shape pick = shapes.front();
+            Shape pick = default_shape(b, mixed, shapes);
             const Shape& t = ctx->tuned[mixed][id];
             if (t.block > 0) {
                 // the tuned shape, or the nearest one that still fits this bucket
