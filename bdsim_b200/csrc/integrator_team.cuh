@@ -167,7 +167,10 @@ static __device__ void tridiag_vec_reg(const double (&a)[kLanczosWarm], const do
     double c[kLanczosWarm];
 #pragma unroll
     for (int i = 0; i < kLanczosWarm; ++i) y[i] = i < m ? y0 : 0.0;
-    for (int it = 0; it < 2; ++it) {
+    // one pass: the shift is within 1e-6 relative of the eigenvalue, so a
+    // single solve already amplifies its eigenvector by ~1e5 over the others
+    // (the vector only seeds the next step's Lanczos)
+    for (int it = 0; it < 1; ++it) {
         // pivots: the reference's tiny-pivot guard (1e-300) raised to 1e-30 so
         // that the reciprocal's single-precision seed stays in range (the
         // vector only seeds the next step's Lanczos)
@@ -501,13 +504,15 @@ struct TeamChain {
     // Fs: spring bead forces (src/spring.cpp:195-207). Fe: (EV + bending) +
     // external(t) (src/model.hpp:56-64). Positions must be staged (S.pos).
     __device__ void forces(const double (&R)[2][3], double t, float (&Fs)[2][3], float (&Fe)[2][3], bool spring) {
-        to_smem(S.s0, R);
+        const bool bend = ch.bend_type != BDCU_BEND_NONE && N > 2;
+        const bool bonds = spring || bend;  // bond forces, unit bonds, lengths: springs and bending only
+        if (bonds) to_smem(S.s0, R);
         sync();
         // bonds b = bead(0), bead(1) (b < N-1): Fc -> s1, unit bonds -> s2, lengths -> s3
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int b = bead(q);
-            if (b < N - 1) {
+            if (bonds && b < N - 1) {
                 const double b0 = S.s0[3 * b + 3] - S.s0[3 * b], b1 = S.s0[3 * b + 4] - S.s0[3 * b + 1],
                              b2 = S.s0[3 * b + 5] - S.s0[3 * b + 2];
                 const double len = clamped_len(b0, b1, b2);
@@ -523,7 +528,6 @@ struct TeamChain {
             }
         }
         sync();
-        const bool bend = ch.bend_type != BDCU_BEND_NONE && N > 2;
         if (bend) {
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
