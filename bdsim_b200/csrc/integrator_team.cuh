@@ -728,14 +728,16 @@ struct TeamChain {
         int k = 0;
         double b = 0.0;
         if (m <= kLanczosWarm) {
-            // warm runs: classical Gram-Schmidt against the whole basis. One
-            // batched team sum per step gives the projections c_u = v_u.w
-            // (u <= j; c_j = alpha_j) and, in the free slot, |w|^2 before the
-            // projection, so beta^2 = |w|^2 - sum c_u^2 (Pythagoras). When the
-            // projections removed all but 1% of |w|^2 (|w'| < 0.1 |w|, the
-            // Daniel-Gragg-Kaufman-Stewart test with eta = 0.1) a second pass
-            // re-orthogonalises and beta comes from an explicit norm. The last
-            // step's beta is not needed (it is not an entry of T).
+            // warm runs (8 steps from the previous step's Ritz vectors): the
+            // three-term recurrence without reorthogonalisation. In 8 FP64
+            // steps the loss of orthogonality (of order eps over the accuracy
+            // of the converged Ritz values) leaves the extreme Ritz values far
+            // inside the 2x / 2% padding of the bounds, and the Chebyshev
+            // fluctuation-dissipation check polices the result. One batched
+            // team sum per step gives alpha = v.w and |w|^2, so beta^2 =
+            // |w|^2 - alpha^2 (Pythagoras, |v| = 1); when that cancels by more
+            // than 99% beta comes from an explicit norm. The last step's beta
+            // is not needed (it is not an entry of T).
             for (int j = 0; j < m; ++j) {
                 store(basis(j, m), v);
                 if (j == 0 && have_dv0) {
@@ -746,81 +748,42 @@ struct TeamChain {
                 } else {
                     apply(v, w);
                 }
-                const bool last = j == m - 1;
+                if (j > 0)
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) w[q][d] -= b * vp[q][d];
                 double c[kLanczosWarm];
-                double ww = 0.0;
+#pragma unroll
+                for (int u = 0; u < kLanczosWarm; ++u) c[u] = 0.0;
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) ww += w[q][d] * w[q][d];
-#pragma unroll
-                for (int u = 0; u < kLanczosWarm; ++u) {
-                    c[u] = (u == kLanczosWarm - 1 && j < kLanczosWarm - 1) ? ww : 0.0;
-                    if (u <= j) {
-                        const double* vu = basis(u, m);
-#pragma unroll
-                        for (int q = 0; q < 2; ++q)
-#pragma unroll
-                            for (int d = 0; d < 3; ++d)
-                                if (valid(q)) c[u] += w[q][d] * vu[3 * bead(q) + d];
+                    for (int d = 0; d < 3; ++d) {
+                        c[0] += v[q][d] * w[q][d];
+                        c[1] += w[q][d] * w[q][d];
                     }
-                }
                 tsum8(c);
-                const double w0sq = c[kLanczosWarm - 1];
-                double al = 0.0, p2 = 0.0;
+                const double al = c[0];
 #pragma unroll
-                for (int u = 0; u < kLanczosWarm; ++u) {
-                    if (u <= j) {
-                        const double* vu = basis(u, m);
+                for (int q = 0; q < 2; ++q)
 #pragma unroll
-                        for (int q = 0; q < 2; ++q)
-#pragma unroll
-                            for (int d = 0; d < 3; ++d)
-                                if (valid(q)) w[q][d] -= c[u] * vu[3 * bead(q) + d];
-                        p2 += c[u] * c[u];
-                    }
-                    if (u == j) al = c[u];
-                }
-                double bsq = w0sq - p2;
-                if (!last && !(bsq >= 0.0101 * p2)) {
-                    double c2[kLanczosWarm];
-#pragma unroll
-                    for (int u = 0; u < kLanczosWarm; ++u) {
-                        c2[u] = 0.0;
-                        if (u <= j) {
-                            const double* vu = basis(u, m);
-#pragma unroll
-                            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                                for (int d = 0; d < 3; ++d)
-                                    if (valid(q)) c2[u] += w[q][d] * vu[3 * bead(q) + d];
-                        }
-                    }
-                    tsum8(c2);
-#pragma unroll
-                    for (int u = 0; u < kLanczosWarm; ++u) {
-                        if (u <= j) {
-                            const double* vu = basis(u, m);
-#pragma unroll
-                            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                                for (int d = 0; d < 3; ++d)
-                                    if (valid(q)) w[q][d] -= c2[u] * vu[3 * bead(q) + d];
-                        }
-                        if (u == j) al += c2[u];
-                    }
-                    bsq = dot(w, w);
-                }
+                    for (int d = 0; d < 3; ++d) w[q][d] -= al * v[q][d];
                 if (tid == 0) S.alpha[k] = al;
                 ++k;
-                if (last) break;
+                if (j == m - 1) break;
+                double bsq = c[1] - al * al;
+                if (!(bsq >= 0.01 * c[1])) bsq = dot(w, w);
                 b = sqrt(bsq);
                 if (b < 1.0e-10) break;
                 const double ib = 1.0 / b;
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) v[q][d] = w[q][d] * ib;
+                    for (int d = 0; d < 3; ++d) {
+                        vp[q][d] = v[q][d];
+                        v[q][d] = w[q][d] * ib;
+                    }
                 if (tid == 0) S.beta[j] = b;
             }
         } else {
