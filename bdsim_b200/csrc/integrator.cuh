@@ -430,18 +430,37 @@ struct Block {
         double* Bs = stage + (int64_t)kk4 * kCholTileStride;  // Bs[k*TS + c] = L(j0 + c, k0 + k)
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
         const int nti = (n - r0 + kCholTile - 1) / kCholTile, ntj = (c1 - c0 + kCholTile - 1) / kCholTile;
+        // Staging loads are issued kStageBatch at a time before their shared
+        // stores, so one memory latency covers a batch instead of each element;
+        // the mixed form's first C fragments are loaded alongside them.
+        constexpr int kStageBatch = 8;
+        const int tot = kk4 * kCholTile;
         for (int t = 0; t < nti * ntj; ++t) {
             const int i0 = r0 + (t / ntj) * kCholTile, j0 = c0 + (t % ntj) * kCholTile;
             if (i0 + kCholTile - 1 < j0) continue;  // all above the diagonal
-            for (int e = threadIdx.x; e < kk4 * kCholTile; e += blockDim.x) {
-                const int k = e / kCholTile, r = e % kCholTile;
-                const bool kin = k < kk;
-                As[k * kCholTileStride + r] = (kin && i0 + r < n) ? L[(int64_t)(k0 + k) * n + i0 + r] : 0.0;
-                Bs[k * kCholTileStride + r] = (kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * n + j0 + r] : 0.0;
+            double cpre[4][2];
+            if constexpr (kMixed) dmma_load_c(warp, i0, j0, c1, lane, nwarps, cpre);
+            for (int e0 = threadIdx.x; e0 < tot; e0 += kStageBatch * blockDim.x) {
+                double va[kStageBatch], vb[kStageBatch];
+#pragma unroll
+                for (int u = 0; u < kStageBatch; ++u) {
+                    const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
+                    const bool kin = e < tot && k < kk;
+                    va[u] = (kin && i0 + r < n) ? L[(int64_t)(k0 + k) * n + i0 + r] : 0.0;
+                    vb[u] = (kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * n + j0 + r] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kStageBatch; ++u) {
+                    const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
+                    if (e < tot) {
+                        As[k * kCholTileStride + r] = va[u];
+                        Bs[k * kCholTileStride + r] = vb[u];
+                    }
+                }
             }
             __syncthreads();
             if constexpr (!kMixed) chol_tile_simt(As, Bs, i0, j0, c1, kk);
-            else chol_tile_dmma(As, Bs, i0, j0, c1, kk4, warp, lane, nwarps);
+            else chol_tile_dmma(As, Bs, i0, j0, c1, kk4, warp, lane, nwarps, cpre);
             __syncthreads();
         }
     }
@@ -540,14 +559,31 @@ struct Block {
 
     // Trailing-update tile on the FP64 tensor cores: the tile is 8x8 blocks
     // of 8x8; warp w takes blocks w, w + nwarps, ..., four at a time (their C
-    // fragments loaded together before the k loop); each block is
+    // fragments loaded together before the k loop; the first four, cpre, by
+    // chol_update before the staging barrier); each block is
     // C += (-A) B over k in steps of 4 with mma.sync.m8n8k4.f64 (A 8x4 row:
     // lane holds A[lane/4][lane%4]; B 4x8 col: lane holds B[lane%4][lane/4];
     // C 8x8: lane holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]).
     // jend: columns from jend on are left alone. kk4: the panel width rounded
     // up to 4 (the staged rows are zero beyond).
+    // C fragments of blocks b0, b0 + nwarps, b0 + 2 nwarps, b0 + 3 nwarps of
+    // the tile at (i0, j0) (zero outside the lower triangle and the matrix).
+    __device__ void dmma_load_c(int b0, int i0, int j0, int jend, int lane, int nwarps, double (&c)[4][2]) {
+        const double* L = Lt;
+        constexpr int B8 = kCholTile / 8;
+        const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int blk = b0 + u * nwarps, tr = (blk % B8) * 8, tc = (blk / B8) * 8;
+            const bool act = blk < B8 * B8 && !(i0 + tr + 7 < j0 + tc);
+            const int i = i0 + tr + g, ja = j0 + tc + 2 * q, jb = ja + 1;
+            c[u][0] = (act && i < n && ja < jend && i >= ja) ? L[(int64_t)ja * n + i] : 0.0;
+            c[u][1] = (act && i < n && jb < jend && i >= jb) ? L[(int64_t)jb * n + i] : 0.0;
+        }
+    }
+
     __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int jend, int kk4, int warp,
-                                   int lane, int nwarps) {
+                                   int lane, int nwarps, const double (&cpre)[4][2]) {
         double* L = Lt;
         constexpr int B8 = kCholTile / 8;
         const int g = lane >> 2, q = lane & 3;
@@ -555,6 +591,12 @@ struct Block {
             double c[4][2];
             int tr[4], tc[4];
             bool act[4], oka[4], okb[4];
+            if (b0 == warp) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) c[u][0] = cpre[u][0], c[u][1] = cpre[u][1];
+            } else {
+                dmma_load_c(b0, i0, j0, jend, lane, nwarps, c);
+            }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int blk = b0 + u * nwarps;
@@ -564,8 +606,6 @@ struct Block {
                 const int i = i0 + tr[u] + g, ja = j0 + tc[u] + 2 * q, jb = ja + 1;
                 oka[u] = act[u] && i < n && ja < jend && i >= ja;
                 okb[u] = act[u] && i < n && jb < jend && i >= jb;
-                c[u][0] = oka[u] ? L[(int64_t)ja * n + i] : 0.0;
-                c[u][1] = okb[u] ? L[(int64_t)jb * n + i] : 0.0;
             }
             for (int k = 0; k < kk4; k += 4) {
 #pragma unroll
