@@ -459,9 +459,34 @@ struct Block {
                 }
             }
             __syncthreads();
+            {  // the next tile's panel rows and C tile into L2 while this one is multiplied
+                int tn = t + 1;
+                while (tn < nti * ntj && r0 + (tn / ntj) * kCholTile + kCholTile - 1 < c0 + (tn % ntj) * kCholTile) ++tn;
+                if (tn < nti * ntj)
+                    prefetch_tile(k0, kk, r0 + (tn / ntj) * kCholTile, c0 + (tn % ntj) * kCholTile, c1);
+            }
             if constexpr (!kMixed) chol_tile_simt(As, Bs, i0, j0, c1, kk);
             else chol_tile_dmma(As, Bs, i0, j0, c1, kk4, warp, lane, nwarps, cpre);
             __syncthreads();
+        }
+    }
+
+    // L2 prefetch hints for the tile at (i0, j0) of chol_update: its staged
+    // panel segments L(i0.., k0 + k) and L(j0.., k0 + k), k < kk, and its C
+    // columns L(i0.., j), j in [j0, min(j0 + kCholTile, c1)). Each 64-element
+    // column segment spans at most five 128-byte lines; one hint goes to
+    // elements 0, 16, 32, 48 and 63 of it (clamped to the matrix).
+    __device__ void prefetch_tile(int k0, int kk, int i0, int j0, int c1) const {
+        const double* L = Lt;
+        const int ncc = c1 - j0 < kCholTile ? c1 - j0 : kCholTile;
+        const int work = (2 * kk + ncc) * 5;
+        for (int w = threadIdx.x; w < work; w += blockDim.x) {
+            const int seg = w / 5, p = w % 5, r = p == 4 ? kCholTile - 1 : p * 16;
+            int col, row;
+            if (seg < kk) col = k0 + seg, row = min(i0 + r, n - 1);
+            else if (seg < 2 * kk) col = k0 + seg - kk, row = min(j0 + r, c1 - 1);
+            else col = j0 + seg - 2 * kk, row = min(i0 + r, n - 1);
+            asm volatile("prefetch.L2 [%0];" ::"l"(L + (int64_t)col * n + row));
         }
     }
 
