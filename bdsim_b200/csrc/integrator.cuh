@@ -439,7 +439,8 @@ struct Block {
             const int i0 = r0 + (t / ntj) * kCholTile, j0 = c0 + (t % ntj) * kCholTile;
             if (i0 + kCholTile - 1 < j0) continue;  // all above the diagonal
             double cpre[4][2];
-            if constexpr (kMixed) dmma_load_c(warp, i0, j0, c1, lane, nwarps, cpre);
+            if constexpr (kMixed)
+                if (warp < kStrips) dmma_load_c(warp, i0, j0, c1, lane, cpre);
             for (int e0 = threadIdx.x; e0 < tot; e0 += kStageBatch * blockDim.x) {
                 double va[kStageBatch], vb[kStageBatch];
 #pragma unroll
@@ -582,25 +583,28 @@ struct Block {
         }
     }
 
-    // Trailing-update tile on the FP64 tensor cores: the tile is 8x8 blocks
-    // of 8x8; warp w takes blocks w, w + nwarps, ..., four at a time (their C
-    // fragments loaded together before the k loop; the first four, cpre, by
-    // chol_update before the staging barrier); each block is
-    // C += (-A) B over k in steps of 4 with mma.sync.m8n8k4.f64 (A 8x4 row:
-    // lane holds A[lane/4][lane%4]; B 4x8 col: lane holds B[lane%4][lane/4];
-    // C 8x8: lane holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]).
-    // jend: columns from jend on are left alone. kk4: the panel width rounded
-    // up to 4 (the staged rows are zero beyond).
-    // C fragments of blocks b0, b0 + nwarps, b0 + 2 nwarps, b0 + 3 nwarps of
-    // the tile at (i0, j0) (zero outside the lower triangle and the matrix).
-    __device__ void dmma_load_c(int b0, int i0, int j0, int jend, int lane, int nwarps, double (&c)[4][2]) {
+    // Trailing-update tile on the FP64 tensor cores. The 64x64 tile is 8x8
+    // blocks of 8x8, grouped in 16 strips of one block-row by four
+    // block-columns (strip s: rows 8 (s % 8), columns 32 (s / 8) + 8u, u < 4);
+    // warp w takes strips w, w + nwarps, ... Per k step of 4 the strip's A
+    // fragment is read once and multiplied into its four C fragments with
+    // mma.sync.m8n8k4.f64, C += (-A) B (A 8x4 row: lane holds
+    // A[lane/4][lane%4]; B 4x8 col: lane holds B[lane%4][lane/4]; C 8x8: lane
+    // holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]). The C fragments of
+    // strip `warp` arrive in cpre (loaded by chol_update before the staging
+    // barrier). jend: columns from jend on are left alone. kk4: the panel
+    // width rounded up to 4 (the staged rows are zero beyond).
+    static constexpr int kStrips = (kCholTile / 8) * (kCholTile / 32);
+
+    // C fragments of strip s of the tile at (i0, j0) (zero outside the lower
+    // triangle and the matrix).
+    __device__ void dmma_load_c(int s, int i0, int j0, int jend, int lane, double (&c)[4][2]) const {
         const double* L = Lt;
-        constexpr int B8 = kCholTile / 8;
-        const int g = lane >> 2, q = lane & 3;
+        const int g = lane >> 2, q = lane & 3, tr = (s % 8) * 8, tcs = (s / 8) * 32;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int blk = b0 + u * nwarps, tr = (blk % B8) * 8, tc = (blk / B8) * 8;
-            const bool act = blk < B8 * B8 && !(i0 + tr + 7 < j0 + tc);
+            const int tc = tcs + 8 * u;
+            const bool act = !(i0 + tr + 7 < j0 + tc);
             const int i = i0 + tr + g, ja = j0 + tc + 2 * q, jb = ja + 1;
             c[u][0] = (act && i < n && ja < jend && i >= ja) ? L[(int64_t)ja * n + i] : 0.0;
             c[u][1] = (act && i < n && jb < jend && i >= jb) ? L[(int64_t)jb * n + i] : 0.0;
@@ -610,34 +614,25 @@ struct Block {
     __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int jend, int kk4, int warp,
                                    int lane, int nwarps, const double (&cpre)[4][2]) {
         double* L = Lt;
-        constexpr int B8 = kCholTile / 8;
         const int g = lane >> 2, q = lane & 3;
-        for (int b0 = warp; b0 < B8 * B8; b0 += 4 * nwarps) {
+        for (int s = warp; s < kStrips; s += nwarps) {
+            const int tr = (s % 8) * 8, tcs = (s / 8) * 32;
+            if (i0 + tr + 7 < j0 + tcs) continue;  // the whole strip above the diagonal (warp-uniform)
             double c[4][2];
-            int tr[4], tc[4];
-            bool act[4], oka[4], okb[4];
-            if (b0 == warp) {
+            if (s == warp) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) c[u][0] = cpre[u][0], c[u][1] = cpre[u][1];
             } else {
-                dmma_load_c(b0, i0, j0, jend, lane, nwarps, c);
+                dmma_load_c(s, i0, j0, jend, lane, c);
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int blk = b0 + u * nwarps;
-                tr[u] = (blk % B8) * 8;
-                tc[u] = (blk / B8) * 8;
-                act[u] = blk < B8 * B8 && !(i0 + tr[u] + 7 < j0 + tc[u]);  // warp-uniform
-                const int i = i0 + tr[u] + g, ja = j0 + tc[u] + 2 * q, jb = ja + 1;
-                oka[u] = act[u] && i < n && ja < jend && i >= ja;
-                okb[u] = act[u] && i < n && jb < jend && i >= jb;
-            }
+            // blocks u < nact are active: the columns grow with u (warp-uniform)
+            const int d = i0 + tr + 7 - j0 - tcs, nact = d >= 24 ? 4 : d / 8 + 1;
             for (int k = 0; k < kk4; k += 4) {
+                const double av = -As[(k + q) * kCholTileStride + tr + g];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    if (act[u]) {
-                        const double av = -As[(k + q) * kCholTileStride + tr[u] + g];
-                        const double bv = Bs[(k + q) * kCholTileStride + tc[u] + g];
+                    if (u < nact) {
+                        const double bv = Bs[(k + q) * kCholTileStride + tcs + 8 * u + g];
                         asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                                      : "+d"(c[u][0]), "+d"(c[u][1])
                                      : "d"(av), "d"(bv));
@@ -646,9 +641,9 @@ struct Block {
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int i = i0 + tr[u] + g, ja = j0 + tc[u] + 2 * q;
-                if (oka[u]) L[(int64_t)ja * n + i] = c[u][0];
-                if (okb[u]) L[(int64_t)(ja + 1) * n + i] = c[u][1];
+                const int i = i0 + tr + g, ja = j0 + tcs + 8 * u + 2 * q, jb = ja + 1;
+                if (u < nact && i < n && ja < jend && i >= ja) L[(int64_t)ja * n + i] = c[u][0];
+                if (u < nact && i < n && jb < jend && i >= jb) L[(int64_t)jb * n + i] = c[u][1];
             }
         }
     }
