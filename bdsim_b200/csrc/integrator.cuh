@@ -431,62 +431,77 @@ struct Block {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
         const int nti = (n - r0 + kCholTile - 1) / kCholTile, ntj = (c1 - c0 + kCholTile - 1) / kCholTile;
         // Staging loads are issued kStageBatch at a time before their shared
-        // stores, so one memory latency covers a batch instead of each element;
-        // the mixed form's first C fragments are loaded alongside them.
+        // stores, so one memory latency covers a batch instead of each element.
+        // The tiles go row by row; the mixed form stages As once per tile-row
+        // (a_i0) and Bs only when its column block changes (b_j0), and a
+        // diagonal tile (i0 == j0) multiplies As by itself (its B rows beyond c1
+        // differ from the zeros Bs would hold, but they only reach C columns >=
+        // c1, which are not stored). The plain form restages both for every
+        // tile: the reuse measured 2.5% slower there (5% faster in the mixed form).
         constexpr int kStageBatch = 8;
-        const int tot = kk4 * kCholTile;
-        for (int t = 0; t < nti * ntj; ++t) {
+        const int tot = kk4 * kCholTile, nt = nti * ntj;
+        auto next_tile = [&](int t) {  // first tile >= t not wholly above the diagonal
+            while (t < nt && r0 + (t / ntj) * kCholTile + kCholTile - 1 < c0 + (t % ntj) * kCholTile) ++t;
+            return t;
+        };
+        int a_i0 = -1, b_j0 = -1;
+        for (int t = next_tile(0); t < nt; t = next_tile(t + 1)) {
             const int i0 = r0 + (t / ntj) * kCholTile, j0 = c0 + (t % ntj) * kCholTile;
-            if (i0 + kCholTile - 1 < j0) continue;  // all above the diagonal
-            double cpre[4][2];
-            if constexpr (kMixed)
-                if (warp < kStrips) dmma_load_c(warp, i0, j0, c1, lane, cpre);
-            for (int e0 = threadIdx.x; e0 < tot; e0 += kStageBatch * blockDim.x) {
-                double va[kStageBatch], vb[kStageBatch];
+            const bool diag = kMixed && i0 == j0, stA = !kMixed || i0 != a_i0, stB = !kMixed || (!diag && j0 != b_j0);
+            a_i0 = i0;
+            if (stB) b_j0 = j0;
+            if (stA || stB) {
+                for (int e0 = threadIdx.x; e0 < tot; e0 += kStageBatch * blockDim.x) {
+                    double va[kStageBatch], vb[kStageBatch];
 #pragma unroll
-                for (int u = 0; u < kStageBatch; ++u) {
-                    const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
-                    const bool kin = e < tot && k < kk;
-                    va[u] = (kin && i0 + r < n) ? L[(int64_t)(k0 + k) * n + i0 + r] : 0.0;
-                    vb[u] = (kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * n + j0 + r] : 0.0;
-                }
+                    for (int u = 0; u < kStageBatch; ++u) {
+                        const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
+                        const bool kin = e < tot && k < kk;
+                        va[u] = (stA && kin && i0 + r < n) ? L[(int64_t)(k0 + k) * n + i0 + r] : 0.0;
+                        vb[u] = (stB && kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * n + j0 + r] : 0.0;
+                    }
 #pragma unroll
-                for (int u = 0; u < kStageBatch; ++u) {
-                    const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
-                    if (e < tot) {
-                        As[k * kCholTileStride + r] = va[u];
-                        Bs[k * kCholTileStride + r] = vb[u];
+                    for (int u = 0; u < kStageBatch; ++u) {
+                        const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
+                        if (e < tot) {
+                            if (stA) As[k * kCholTileStride + r] = va[u];
+                            if (stB) Bs[k * kCholTileStride + r] = vb[u];
+                        }
                     }
                 }
             }
             __syncthreads();
-            {  // the next tile's panel rows and C tile into L2 while this one is multiplied
-                int tn = t + 1;
-                while (tn < nti * ntj && r0 + (tn / ntj) * kCholTile + kCholTile - 1 < c0 + (tn % ntj) * kCholTile) ++tn;
-                if (tn < nti * ntj)
-                    prefetch_tile(k0, kk, r0 + (tn / ntj) * kCholTile, c0 + (tn % ntj) * kCholTile, c1);
+            {  // the next tile's new panel rows and its C tile into L2 while this one is multiplied
+                const int tn = next_tile(t + 1);
+                if (tn < nt) {
+                    const int i1 = r0 + (tn / ntj) * kCholTile, j1 = c0 + (tn % ntj) * kCholTile;
+                    prefetch_tile(k0, kk, i1, j1, c1, !kMixed || i1 != i0, !kMixed || (i1 != j1 && j1 != b_j0));
+                }
             }
-            if constexpr (!kMixed) chol_tile_simt(As, Bs, i0, j0, c1, kk);
-            else chol_tile_dmma(As, Bs, i0, j0, c1, kk4, warp, lane, nwarps, cpre);
+            const double* Bt = diag ? As : Bs;
+            if constexpr (!kMixed) chol_tile_simt(As, Bt, i0, j0, c1, kk);
+            else chol_tile_dmma(As, Bt, i0, j0, c1, kk4, warp, lane, nwarps);
             __syncthreads();
         }
     }
 
     // L2 prefetch hints for the tile at (i0, j0) of chol_update: its staged
-    // panel segments L(i0.., k0 + k) and L(j0.., k0 + k), k < kk, and its C
-    // columns L(i0.., j), j in [j0, min(j0 + kCholTile, c1)). Each 64-element
-    // column segment spans at most five 128-byte lines; one hint goes to
-    // elements 0, 16, 32, 48 and 63 of it (clamped to the matrix).
-    __device__ void prefetch_tile(int k0, int kk, int i0, int j0, int c1) const {
+    // panel segments L(i0.., k0 + k) (if wantA) and L(j0.., k0 + k) (if
+    // wantB), k < kk, and its C columns L(i0.., j), j in [j0, min(j0 +
+    // kCholTile, c1)). Each 64-element column segment spans at most five
+    // 128-byte lines; one hint goes to elements 0, 16, 32, 48 and 63 of it
+    // (clamped to the matrix).
+    __device__ void prefetch_tile(int k0, int kk, int i0, int j0, int c1, bool wantA, bool wantB) const {
         const double* L = Lt;
+        const int na = wantA ? kk : 0, nb = wantB ? kk : 0;
         const int ncc = c1 - j0 < kCholTile ? c1 - j0 : kCholTile;
-        const int work = (2 * kk + ncc) * 5;
+        const int work = (na + nb + ncc) * 5;
         for (int w = threadIdx.x; w < work; w += blockDim.x) {
             const int seg = w / 5, p = w % 5, r = p == 4 ? kCholTile - 1 : p * 16;
             int col, row;
-            if (seg < kk) col = k0 + seg, row = min(i0 + r, n - 1);
-            else if (seg < 2 * kk) col = k0 + seg - kk, row = min(j0 + r, c1 - 1);
-            else col = j0 + seg - 2 * kk, row = min(i0 + r, n - 1);
+            if (seg < na) col = k0 + seg, row = min(i0 + r, n - 1);
+            else if (seg < na + nb) col = k0 + seg - na, row = min(j0 + r, c1 - 1);
+            else col = j0 + seg - na - nb, row = min(i0 + r, n - 1);
             asm volatile("prefetch.L2 [%0];" ::"l"(L + (int64_t)col * n + row));
         }
     }
@@ -590,10 +605,11 @@ struct Block {
     // fragment is read once and multiplied into its four C fragments with
     // mma.sync.m8n8k4.f64, C += (-A) B (A 8x4 row: lane holds
     // A[lane/4][lane%4]; B 4x8 col: lane holds B[lane%4][lane/4]; C 8x8: lane
-    // holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]). The C fragments of
-    // strip `warp` arrive in cpre (loaded by chol_update before the staging
-    // barrier). jend: columns from jend on are left alone. kk4: the panel
-    // width rounded up to 4 (the staged rows are zero beyond).
+    // holds C[lane/4][2(lane%4)], C[lane/4][2(lane%4)+1]). (Loading the first
+    // strip's C fragments before the staging barrier instead made the kernel
+    // spill at its 128-register cap and measured 3% slower.) jend: columns
+    // from jend on are left alone. kk4: the panel width rounded up to 4 (the
+    // staged rows are zero beyond).
     static constexpr int kStrips = (kCholTile / 8) * (kCholTile / 32);
 
     // C fragments of strip s of the tile at (i0, j0) (zero outside the lower
@@ -612,19 +628,14 @@ struct Block {
     }
 
     __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int jend, int kk4, int warp,
-                                   int lane, int nwarps, const double (&cpre)[4][2]) {
+                                   int lane, int nwarps) {
         double* L = Lt;
         const int g = lane >> 2, q = lane & 3;
         for (int s = warp; s < kStrips; s += nwarps) {
             const int tr = (s % 8) * 8, tcs = (s / 8) * 32;
             if (i0 + tr + 7 < j0 + tcs) continue;  // the whole strip above the diagonal (warp-uniform)
             double c[4][2];
-            if (s == warp) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) c[u][0] = cpre[u][0], c[u][1] = cpre[u][1];
-            } else {
-                dmma_load_c(s, i0, j0, jend, lane, c);
-            }
+            dmma_load_c(s, i0, j0, jend, lane, c);
             // blocks u < nact are active: the columns grow with u (warp-uniform)
             const int d = i0 + tr + 7 - j0 - tcs, nact = d >= 24 ? 4 : d / 8 + 1;
             for (int k = 0; k < kk4; k += 4) {

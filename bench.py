@@ -468,7 +468,7 @@ def main():
         barrier()
         r["total_ms"] = reduce_max(sum(r["ms"]), dist, device="cuda")
         results["mixed_k4"] = r
-    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), 1, first, "mixed")
+    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), max(3, args.warmup), first, "mixed")
     serving = None
     if args.serving_seconds > 0 and set(forms) == {"plain", "mixed"}:
         serving = run_serving(torch, args.serving_seconds, seed=rank)
