@@ -426,6 +426,11 @@ struct Block {
     __device__ void chol_update(int k0, int k1, int r0, int c0, int c1) {
         double* L = Lt;
         const int kk = k1 - k0, kk4 = (kk + 3) & ~3;  // staged rows k >= kk are zero
+        if constexpr (!kMixed)
+            if (blockDim.x == 512 && (int64_t)3 * kk4 * kCholTile <= stage_cap) {
+                chol_update_pairs(k0, k1, r0, c0, c1);
+                return;
+            }
         double* As = stage;                                   // As[k*TS + r] = L(i0 + r, k0 + k)
         double* Bs = stage + (int64_t)kk4 * kCholTileStride;  // Bs[k*TS + c] = L(j0 + c, k0 + k)
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -479,9 +484,61 @@ struct Block {
                 }
             }
             const double* Bt = diag ? As : Bs;
-            if constexpr (!kMixed) chol_tile_simt(As, Bt, i0, j0, c1, kk);
+            if constexpr (!kMixed) chol_tile_simt<kCholTileStride>(As, Bt, i0, j0, c1, kk, threadIdx.x, blockDim.x);
             else chol_tile_dmma(As, Bt, i0, j0, c1, kk4, warp, lane, nwarps);
             __syncthreads();
+        }
+    }
+
+    // chol_update for the plain form with 512 threads: a 4x4 micro-tile per
+    // thread covers 256 threads of a tile, so each pass takes two tiles of a
+    // tile-row, (i0, j0) for threads 0-255 and (i0, j0 + 64) for 256-511,
+    // against one staged As and two Bs. The three buffers are unpadded
+    // (every access to them runs along a row). Each element still receives
+    // its products in k order: the arithmetic is the single-tile path's.
+    __device__ void chol_update_pairs(int k0, int k1, int r0, int c0, int c1) {
+        const double* L = Lt;
+        constexpr int TS = kCholTile;
+        const int kk = k1 - k0, kk4 = (kk + 3) & ~3, tot = kk4 * kCholTile;
+        double* As = stage;
+        double* B0 = stage + (int64_t)kk4 * TS;
+        double* B1 = B0 + (int64_t)kk4 * TS;
+        const int nti = (n - r0 + kCholTile - 1) / kCholTile, ntj = (c1 - c0 + kCholTile - 1) / kCholTile;
+        const int half = threadIdx.x >> 8, hl = threadIdx.x & 255;
+        constexpr int kB = 4;  // staged elements per thread per array between loads and stores
+        for (int ti = 0; ti < nti; ++ti) {
+            const int i0 = r0 + ti * kCholTile;
+            // tiles (ti, tj) with tj < tjn reach the diagonal (r0 == c0 in both callers, so i0 >= c0)
+            const int tjn = min(ntj, (i0 + kCholTile - 1 - c0) / kCholTile + 1);
+            for (int tj = 0; tj < tjn; tj += 2) {
+                const int j0 = c0 + tj * kCholTile, j1 = j0 + kCholTile;
+                const bool two = tj + 1 < tjn;
+                for (int e0 = threadIdx.x; e0 < tot; e0 += kB * blockDim.x) {
+                    double va[kB], v0[kB], v1[kB];
+#pragma unroll
+                    for (int u = 0; u < kB; ++u) {
+                        const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
+                        const bool kin = e < tot && k < kk;
+                        const double* col = L + (int64_t)(k0 + k) * n;
+                        va[u] = (kin && i0 + r < n) ? col[i0 + r] : 0.0;
+                        v0[u] = (kin && j0 + r < c1) ? col[j0 + r] : 0.0;
+                        v1[u] = (two && kin && j1 + r < c1) ? col[j1 + r] : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kB; ++u) {
+                        const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
+                        if (e < tot) {
+                            As[k * TS + r] = va[u];
+                            B0[k * TS + r] = v0[u];
+                            if (two) B1[k * TS + r] = v1[u];
+                        }
+                    }
+                }
+                __syncthreads();
+                if (half == 0) chol_tile_simt<TS>(As, B0, i0, j0, c1, kk, hl, 256);
+                else if (two) chol_tile_simt<TS>(As, B1, i0, j1, c1, kk, hl, 256);
+                __syncthreads();
+            }
         }
     }
 
@@ -563,10 +620,14 @@ struct Block {
     // Trailing-update tile, FP64 CUDA cores: 4x4 elements per thread, each
     // element c = c - a_k * b_k for k = 0, 1, ... (no contraction: the plain
     // form is compiled without FMA).
-    __device__ void chol_tile_simt(const double* As, const double* Bs, int i0, int j0, int jend, int kk) {
+    // Threads take micro-tiles first, first + step, ...; As / Bs rows are TS
+    // doubles apart.
+    template <int TS>
+    __device__ void chol_tile_simt(const double* As, const double* Bs, int i0, int j0, int jend, int kk, int first,
+                                   int step) {
         double* L = Lt;
         constexpr int Q = kCholTile / 4;
-        for (int mtl = threadIdx.x; mtl < Q * Q; mtl += blockDim.x) {
+        for (int mtl = first; mtl < Q * Q; mtl += step) {
             const int r0 = (mtl % Q) * 4, c0 = (mtl / Q) * 4;
             if (i0 + r0 + 3 < j0 + c0) continue;  // all above the diagonal
             double c[4][4];
@@ -578,10 +639,10 @@ struct Block {
                     c[u][v] = (i < n && j < jend && i >= j) ? L[(int64_t)j * n + i] : 0.0;
                 }
             for (int k = 0; k < kk; ++k) {
-                const double2 a01 = *reinterpret_cast<const double2*>(As + k * kCholTileStride + r0);
-                const double2 a23 = *reinterpret_cast<const double2*>(As + k * kCholTileStride + r0 + 2);
-                const double2 b01 = *reinterpret_cast<const double2*>(Bs + k * kCholTileStride + c0);
-                const double2 b23 = *reinterpret_cast<const double2*>(Bs + k * kCholTileStride + c0 + 2);
+                const double2 a01 = *reinterpret_cast<const double2*>(As + k * TS + r0);
+                const double2 a23 = *reinterpret_cast<const double2*>(As + k * TS + r0 + 2);
+                const double2 b01 = *reinterpret_cast<const double2*>(Bs + k * TS + c0);
+                const double2 b23 = *reinterpret_cast<const double2*>(Bs + k * TS + c0 + 2);
                 const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
