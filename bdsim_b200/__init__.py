@@ -12,7 +12,7 @@ from .params import (Spring, EV, Bending, DelSMethod, SpringParams, EVParams, Be
 from .core import (integrate, integrate_many, total_force, total_force_many, spring_force, bending_force,
                    ev_force, external_force, IntegratorError)
 from .engine import Context, Ensemble
-from . import flows, initial, properties, storage, parallel, ensemble
+from . import flows, initial, properties, storage, parallel, ensemble, rheology
 from .initial import (gaussian_chain, fene_fraenkel_chain, fene_fraenkel_chain_aligned_x, equilibrium_chain,
                       fene_fraenkel_bending_chain, one_minus_cos_theta_angles, isotropic_directions)
 from .properties import (end_to_end_sq, radius_of_gyration_sq, gyration_tensor, stretch, kramers_stress,
@@ -26,7 +26,7 @@ __all__ = [
     "Spring", "EV", "Bending", "DelSMethod", "SpringParams", "EVParams", "BendingParams", "PhysParams",
     "SimParams", "Flow", "Rng", "ExternalForce", "integrate", "integrate_many", "total_force",
     "total_force_many", "spring_force", "bending_force", "ev_force", "external_force", "IntegratorError",
-    "Context", "Ensemble", "flows", "initial", "properties", "storage", "parallel", "ensemble",
+    "Context", "Ensemble", "flows", "initial", "properties", "storage", "parallel", "ensemble", "rheology",
     "gaussian_chain", "fene_fraenkel_chain", "fene_fraenkel_chain_aligned_x", "equilibrium_chain",
     "fene_fraenkel_bending_chain", "one_minus_cos_theta_angles", "isotropic_directions",
     "end_to_end_sq", "radius_of_gyration_sq", "gyration_tensor", "stretch", "kramers_stress",

@@ -19,7 +19,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import storage
+from . import rheology, storage
 from ._abi import CACHE_PERSIST, CACHE_RESET_PER_CALL, ST_FATAL_MASK, count_steps
 from .core import IntegratorError, integrate
 from .engine import Ensemble
@@ -212,10 +212,12 @@ def run_ensemble(phys: PhysParams, sim: SimParams, n_traj: int, per_trajectory, 
                  max_failed_fraction=None, form="plain", device: int = 0):
     """Run n_traj chains, reducing each with per_trajectory (ensemble.py:330-379).
 
-    final_state and sampled_states run batched: all trajectories advance
-    together in one device batch per integrate segment. Any other function is
-    called once per trajectory as per_trajectory(R0, phys, sim, rng, *args);
-    the integrate calls it makes run on the GPU one chain at a time.
+    final_state, sampled_states and the rheology series (stress_series,
+    viscosity_series, viscosity_series_vr) run batched: all trajectories
+    (and the control chains of the variance-reduced series) advance together
+    in one device batch per integrate segment. Any other function is called
+    once per trajectory as per_trajectory(R0, phys, sim, rng, *args); the
+    integrate calls it makes run on the GPU one chain at a time.
     """
     _check_backend(backend)
     initial = initial or Initial()
@@ -239,6 +241,10 @@ def run_ensemble(phys: PhysParams, sim: SimParams, n_traj: int, per_trajectory, 
                 out.append(Failure(i, IntegratorError(int(status[i]), i)))
             else:
                 out.append(per[i][-1] if per_trajectory is final_state else per[i])
+    elif per_trajectory in rheology.BATCHED:
+        R0s = [INITIALIZERS[initial.method](phys.number_of_beads, seed + i, dict(initial.kwargs))
+               for i in range(n_traj)]
+        out = rheology.run_batched(per_trajectory, phys, sim, n_traj, args, R0s, seed, form, device)
     else:
         out = []
         for i in range(n_traj):
