@@ -699,7 +699,31 @@ struct Block {
             dmma_load_c(s, i0, j0, jend, lane, c);
             // blocks u < nact are active: the columns grow with u (warp-uniform)
             const int d = i0 + tr + 7 - j0 - tcs, nact = d >= 24 ? 4 : d / 8 + 1;
-            for (int k = 0; k < kk4; k += 4) {
+            // Two accumulation chains per fragment (k steps alternate between c
+            // and c2, summed at the end) halve the dependent-DMMA wait; the
+            // mixed form's tolerance admits the reassociation.
+            double c2[4][2];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) c2[u][0] = c2[u][1] = 0.0;
+            int k = 0;
+            for (; k + 8 <= kk4; k += 8) {
+                const double av = -As[(k + q) * kCholTileStride + tr + g];
+                const double av2 = -As[(k + 4 + q) * kCholTileStride + tr + g];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (u < nact) {
+                        const double bv = Bs[(k + q) * kCholTileStride + tcs + 8 * u + g];
+                        const double bv2 = Bs[(k + 4 + q) * kCholTileStride + tcs + 8 * u + g];
+                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                     : "+d"(c[u][0]), "+d"(c[u][1])
+                                     : "d"(av), "d"(bv));
+                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                     : "+d"(c2[u][0]), "+d"(c2[u][1])
+                                     : "d"(av2), "d"(bv2));
+                    }
+                }
+            }
+            if (k < kk4) {  // kk4 is a multiple of 4: one step left
                 const double av = -As[(k + q) * kCholTileStride + tr + g];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
@@ -711,6 +735,8 @@ struct Block {
                     }
                 }
             }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) c[u][0] += c2[u][0], c[u][1] += c2[u][1];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = i0 + tr + g, ja = j0 + tcs + 8 * u + 2 * q, jb = ja + 1;
