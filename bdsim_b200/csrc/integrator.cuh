@@ -535,6 +535,15 @@ struct Block {
                     }
                 }
                 __syncthreads();
+                {  // the next pass's panel rows and C tiles into L2 while this one is multiplied
+                    int ti1 = ti, tj1 = tj + 2;
+                    if (tj1 >= tjn) ti1 = ti + 1, tj1 = 0;
+                    if (ti1 < nti) {
+                        const int i1 = r0 + ti1 * kCholTile, n1 = min(ntj, (i1 + kCholTile - 1 - c0) / kCholTile + 1);
+                        prefetch_tile(k0, kk, i1, c0 + tj1 * kCholTile, c1, true, true);
+                        if (tj1 + 1 < n1) prefetch_tile(k0, kk, i1, c0 + (tj1 + 1) * kCholTile, c1, false, true);
+                    }
+                }
                 if (half == 0) chol_tile_simt<TS>(As, B0, i0, j0, c1, kk, hl, 256);
                 else if (two) chol_tile_simt<TS>(As, B1, i0, j1, c1, kk, hl, 256);
                 __syncthreads();
@@ -699,36 +708,39 @@ struct Block {
             dmma_load_c(s, i0, j0, jend, lane, c);
             // blocks u < nact are active: the columns grow with u (warp-uniform)
             const int d = i0 + tr + 7 - j0 - tcs, nact = d >= 24 ? 4 : d / 8 + 1;
-            // Two accumulation chains per fragment (k steps alternate between c
-            // and c2, summed at the end) halve the dependent-DMMA wait; the
+            // kDmmaChains accumulation chains per fragment (k steps rotate over
+            // c and cx, summed at the end) cut the dependent-DMMA wait; the
             // mixed form's tolerance admits the reassociation.
-            double c2[4][2];
+            constexpr int kDmmaChains = 4;
+            double cx[kDmmaChains - 1][4][2];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) c2[u][0] = c2[u][1] = 0.0;
+            for (int h = 0; h < kDmmaChains - 1; ++h)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) cx[h][u][0] = cx[h][u][1] = 0.0;
             int k = 0;
-            for (; k + 8 <= kk4; k += 8) {
+            for (; k + 4 * kDmmaChains <= kk4; k += 4 * kDmmaChains) {
+#pragma unroll
+                for (int h = 0; h < kDmmaChains; ++h) {
+                    const double av = -As[(k + 4 * h + q) * kCholTileStride + tr + g];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        if (u < nact) {
+                            const double bv = Bs[(k + 4 * h + q) * kCholTileStride + tcs + 8 * u + g];
+                            double& d0 = h == 0 ? c[u][0] : cx[h > 0 ? h - 1 : 0][u][0];
+                            double& d1 = h == 0 ? c[u][1] : cx[h > 0 ? h - 1 : 0][u][1];
+                            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                         : "+d"(d0), "+d"(d1)
+                                         : "d"(av), "d"(bv));
+                        }
+                    }
+                }
+            }
+            for (; k < kk4; k += 4) {  // kk4 is a multiple of 4
                 const double av = -As[(k + q) * kCholTileStride + tr + g];
-                const double av2 = -As[(k + 4 + q) * kCholTileStride + tr + g];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     if (u < nact) {
                         const double bv = Bs[(k + q) * kCholTileStride + tcs + 8 * u + g];
-                        const double bv2 = Bs[(k + 4 + q) * kCholTileStride + tcs + 8 * u + g];
-                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                                     : "+d"(c[u][0]), "+d"(c[u][1])
-                                     : "d"(av), "d"(bv));
-                        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                                     : "+d"(c2[u][0]), "+d"(c2[u][1])
-                                     : "d"(av2), "d"(bv2));
-                    }
-                }
-            }
-            if (k < kk4) {  // kk4 is a multiple of 4: one step left
-                const double av = -As[(k + q) * kCholTileStride + tr + g];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    if (u < nact) {
-                        const double bv = Bs[(k + q) * kCholTileStride + tcs + 8 * u + g];
                         asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                                      : "+d"(c[u][0]), "+d"(c[u][1])
                                      : "d"(av), "d"(bv));
@@ -736,7 +748,9 @@ struct Block {
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) c[u][0] += c2[u][0], c[u][1] += c2[u][1];
+            for (int h = 0; h < kDmmaChains - 1; ++h)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) c[u][0] += cx[h][u][0], c[u][1] += cx[h][u][1];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = i0 + tr + g, ja = j0 + tcs + 8 * u + 2 * q, jb = ja + 1;
