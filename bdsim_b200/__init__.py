@@ -12,7 +12,7 @@ from .params import (Spring, EV, Bending, DelSMethod, SpringParams, EVParams, Be
 from .core import (integrate, integrate_many, total_force, total_force_many, spring_force, bending_force,
                    ev_force, external_force, IntegratorError)
 from .engine import Context, Ensemble
-from . import flows, initial, properties, storage, parallel, ensemble, rheology
+from . import flows, initial, properties, storage, failures, ensemble, rheology
 from .initial import (gaussian_chain, fene_fraenkel_chain, fene_fraenkel_chain_aligned_x, equilibrium_chain,
                       fene_fraenkel_bending_chain, one_minus_cos_theta_angles, isotropic_directions)
 from .properties import (end_to_end_sq, radius_of_gyration_sq, gyration_tensor, stretch, kramers_stress,
@@ -20,18 +20,18 @@ from .properties import (end_to_end_sq, radius_of_gyration_sq, gyration_tensor, 
 from .ensemble import (Initial, Output, INITIALIZERS, n_steps_of, simulate, run_ensemble, trajectory_samples,
                        final_state, sampled_states, mean_stderr, MAX_FAILED_FRACTION)
 from .storage import read_run, read_trajectory, Run, Trajectory, map_property, ensemble_average
-from .parallel import parallel_map, Failure
+from .failures import Failure
 
 __all__ = [
     "Spring", "EV", "Bending", "DelSMethod", "SpringParams", "EVParams", "BendingParams", "PhysParams",
     "SimParams", "Flow", "Rng", "ExternalForce", "integrate", "integrate_many", "total_force",
     "total_force_many", "spring_force", "bending_force", "ev_force", "external_force", "IntegratorError",
-    "Context", "Ensemble", "flows", "initial", "properties", "storage", "parallel", "ensemble", "rheology",
+    "Context", "Ensemble", "flows", "initial", "properties", "storage", "failures", "ensemble", "rheology",
     "gaussian_chain", "fene_fraenkel_chain", "fene_fraenkel_chain_aligned_x", "equilibrium_chain",
     "fene_fraenkel_bending_chain", "one_minus_cos_theta_angles", "isotropic_directions",
     "end_to_end_sq", "radius_of_gyration_sq", "gyration_tensor", "stretch", "kramers_stress",
     "shear_viscosity_config", "normal_stress_differences", "Initial", "Output", "INITIALIZERS", "n_steps_of",
     "simulate", "run_ensemble", "trajectory_samples", "final_state", "sampled_states", "mean_stderr",
     "MAX_FAILED_FRACTION", "read_run", "read_trajectory", "Run", "Trajectory", "map_property",
-    "ensemble_average", "parallel_map", "Failure",
+    "ensemble_average", "Failure",
 ]

@@ -10,7 +10,7 @@ import os
 
 import numpy as np
 
-from .params import PhysParams, SimParams
+from .params import PhysParams, SimParams, external_entries
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
 c_int32_p = ctypes.POINTER(ctypes.c_int32)
@@ -122,13 +122,19 @@ class _Arena:
         return np.concatenate(self.chunks)
 
 
+def _code(v) -> int:
+    """Integer code of an enum value: this package's IntEnums, or the
+    reference's nanobind enums (enum.Enum subclasses whose int is `.value`)."""
+    return int(getattr(v, "value", v))
+
+
 def _fill_phys(rec: BdcuPhys, phys: PhysParams, n_beads: int, arena: _Arena):
     rec.n_beads = int(n_beads)
-    rec.spring_type = int(phys.spring.type)
+    rec.spring_type = _code(phys.spring.type)
     rec.sqrtb = float(phys.spring.sqrtb)
     rec.natural_length = float(phys.spring.natural_length)
     ev = phys.ev
-    rec.ev_type = int(ev.type)
+    rec.ev_type = _code(ev.type)
     rec.contour_dist_for_ev = int(ev.contour_dist_for_EV)
     rec.zstar = float(ev.zstar)
     rec.dstar = float(ev.dstar)
@@ -140,24 +146,28 @@ def _fill_phys(rec: BdcuPhys, phys: PhysParams, n_beads: int, arena: _Arena):
         if phi.size != n_beads * n_beads:
             raise ValueError(f"EVParams.phi must hold N*N={n_beads * n_beads} values, got {phi.size}")
         rec.phi_offset = arena.add(phi, key=("phi", phi.tobytes()))
-    rec.bend_type = int(phys.bend.type)
+    rec.bend_type = _code(phys.bend.type)
     rec.equilibration = int(bool(phys.equilibration))
     rec.bend_stiffness = float(phys.bend.stiffness)
     rec.hstar = float(phys.hstar)
-    rec.hi_method = int(phys.hi_method)
+    rec.hi_method = _code(phys.hi_method)
     rec.ncheb_multiplier = float(phys.ncheb_multiplier)
     rec.fd_err_max = float(phys.fd_err_max)
-    fl = phys.flow
-    for i, v in enumerate(np.asarray(fl._k0, dtype=np.float64).reshape(-1)):
+    # Flow and ExternalForce are read through their pickled state, whose layout
+    # this package shares with the reference's nanobind objects
+    # (bindings/module.cpp:83-99 and 140-148), so either package's objects pack.
+    constant, k0, times, ks = phys.flow.__getstate__()
+    for i, v in enumerate(np.asarray(k0, dtype=np.float64).reshape(-1)):
         rec.flow_kappa[i] = float(v)
-    if fl.is_constant():
+    times = np.asarray(times, dtype=np.float64).reshape(-1)
+    ks = np.asarray(ks, dtype=np.float64).reshape(-1)
+    if constant or times.size == 0:
         rec.flow_n_times = 0
         rec.flow_offset = 0
     else:
-        rec.flow_n_times = len(fl._times)
-        rec.flow_offset = arena.add(np.concatenate([fl._times, fl._ks.reshape(-1)]),
-                                    key=("flow", fl._times.tobytes(), fl._ks.tobytes()))
-    ents = phys.external.entries()
+        rec.flow_n_times = int(times.size)
+        rec.flow_offset = arena.add(np.concatenate([times, ks]), key=("flow", times.tobytes(), ks.tobytes()))
+    ents = list(external_entries(phys.external.__getstate__()))
     rec.ext_n_entries = len(ents)
     rec.ext_offset = 0
     if ents:
@@ -203,7 +213,7 @@ def pack_batch(phys_list, sim_list, n_beads_list):
 
 def count_steps(sim: SimParams) -> int:
     """Steps the reference loop `for (t = t0; t <= t1 + dt/2; t += dt)`
-    takes (src/integrator.cpp:102), replayed in double arithmetic."""
+    takes (src/integrator.cpp:67), replayed in double arithmetic."""
     t, t1, dt = float(sim.time_start), float(sim.time_end), float(sim.dt)
     if not dt > 0.0:
         raise ValueError("dt must be positive")
@@ -273,7 +283,9 @@ def load_library():
                                        ctypes.POINTER(BdcuSim), c_int64_p]
     lib.bdcu_write_arena.argtypes = [vp, ctypes.c_int64, c_double_p, ctypes.c_int64]
     lib.bdcu_select.argtypes = [vp, ctypes.c_int, c_int32_p]
-    for name in ("bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
+    lib.bdcu_check_chains.argtypes = [ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim), c_double_p,
+                                      ctypes.c_int64, ctypes.c_char_p, ctypes.c_int]
+    for name in ("bdcu_check_chains", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
                  "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
                  "bdcu_forces", "bdcu_ran1", "bdcu_run_static", "bdcu_describe_plan", "bdcu_autotune",
                  "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select"):
@@ -288,7 +300,16 @@ EXPORTED_SYMBOLS = [
     "bdcu_set_chains", "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host",
     "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_describe_plan", "bdcu_autotune",
     "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select", "bdcu_run_static",
+    "bdcu_check_chains",
 ]
+
+
+def check_records(n, phys_arr, sim_arr, arena):
+    """bdcu_check_chains on packed records (no GPU needed) -> (status, message)."""
+    lib = load_library()
+    msg = ctypes.create_string_buffer(512)
+    rc = lib.bdcu_check_chains(n, phys_arr, sim_arr, arena.ctypes.data_as(c_double_p), arena.size, msg, 512)
+    return rc, msg.value.decode()
 
 KERNEL_BLOCK, KERNEL_TEAM = 0, 1
 MAX_BUCKETS = 8

@@ -18,7 +18,7 @@ import numpy as np
 from . import _abi
 from ._abi import ST_FATAL_MASK, STATUS_NAMES
 from .engine import Context, form_code
-from .params import PhysParams, SimParams
+from .params import PhysParams, SimParams, rng_state, set_rng_state
 
 _local = threading.local()
 
@@ -54,12 +54,12 @@ def integrate_many(Rs, phys, sims, rngs, *, form="plain", device: int = 0, raise
     sims_l = sims if isinstance(sims, (list, tuple)) else [sims] * n
     Ns = [len(r) for r in Rs]
     R = np.ascontiguousarray(np.concatenate([np.asarray(r, dtype=np.float64).reshape(-1, 3) for r in Rs]))
-    rng = np.ascontiguousarray(np.array([g.state() for g in rngs], dtype=np.int32).reshape(n, 3))
+    rng = np.ascontiguousarray(np.array([rng_state(g) for g in rngs], dtype=np.int32).reshape(n, 3))
     ctx = _ctx(device)
     ctx.set_chains(phys_l, sims_l, Ns)
     status, counters = ctx.integrate_host(R, rng, form_code(form))
     for g, st in zip(rngs, rng):
-        g.set_state(st)
+        set_rng_state(g, st)
     off = np.concatenate([[0], np.cumsum(Ns)])
     out = [R[off[i]:off[i + 1]].copy() for i in range(n)]
     if raise_on_failure:

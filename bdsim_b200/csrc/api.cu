@@ -591,6 +591,26 @@ int bdcu_set_stream(bdcu_ctx* ctx, void* stream) {
 
 const char* bdcu_last_error(bdcu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int bdcu_check_chains(int n_chains, const bdcu_phys* phys, const bdcu_sim* sim, const double* arena,
+                      int64_t arena_len, char* msg, int msg_len) {
+    bdcu_ctx scratch;
+    int rc = BDCU_OK;
+    if (n_chains < 1 || !phys || !sim) {
+        rc = fail(&scratch, BDCU_E_ARG, "need n_chains >= 1 and phys/sim records");
+    } else if (arena_len < 0 || (arena_len > 0 && !arena)) {
+        rc = fail(&scratch, BDCU_E_ARG, "bad arena");
+    } else {
+        for (int i = 0; i < n_chains && rc == BDCU_OK; ++i)
+            rc = validate(&scratch, i, phys[i], sim[i], arena, arena_len);
+    }
+    if (msg && msg_len > 0) {
+        const size_t n = std::min<size_t>(scratch.err.size(), (size_t)msg_len - 1);
+        memcpy(msg, scratch.err.data(), n);
+        msg[n] = '\0';
+    }
+    return rc;
+}
+
 int bdcu_count_steps(const bdcu_sim* sim, int64_t* n_steps_out) {
     if (!sim || !n_steps_out || !(sim->dt > 0.0)) return BDCU_E_ARG;
     int64_t n = 0;
@@ -1042,6 +1062,13 @@ int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double
 }  // extern "C"
 
 namespace bdcu {
+// The checks bdcu_set_chains makes on one chain record, for the static-scratch
+// entry point (so both entry points accept the same inputs).
+int validate_chain(bdcu_ctx* ctx, int i, const bdcu_phys& p, const bdcu_sim& s, const double* arena,
+                   int64_t arena_len) {
+    return validate(ctx, i, p, s, arena, arena_len);
+}
+
 // The per-chain record derivation, for the static-scratch entry point.
 DevChain derive_record(const bdcu_phys& p, const bdcu_sim& s, int64_t bead_off) {
     double ss = 0.0;

@@ -8,8 +8,8 @@
 namespace bdcu {
 
 constexpr int kMaxCheb = 500;      // MAXCHEB (src/types.hpp:20)
-constexpr int kLanczosCold = 30;   // src/hydrodynamics.cpp:134
-constexpr int kLanczosWarm = 8;    // src/hydrodynamics.cpp:135
+constexpr int kLanczosCold = 30;   // src/hydrodynamics.cpp:79
+constexpr int kLanczosWarm = 8;    // src/hydrodynamics.cpp:80
 constexpr int kMaxBeads = 4096;    // largest chain a launch accepts
 
 // Per-chain record derived on the host from bdcu_phys/bdcu_sim. Constants the

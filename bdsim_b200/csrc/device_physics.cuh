@@ -208,7 +208,7 @@ __device__ inline int rtsafe_wlcb(double dt, double s, double gama, double x1, d
     return BDCU_ST_RTSAFE_FAIL;
 }
 
-// solve_implicit_r(...).length (src/spring.cpp:174-223) -- the force factor
+// solve_implicit_r(...).length (src/spring.cpp:123-172) -- the force factor
 // it also returns is unused by solve_connector and not computed here.
 __device__ inline double implicit_length(int type, double dtby4, double gama, double natscl, int& st) {
     switch (type) {
@@ -246,7 +246,7 @@ __device__ inline double implicit_length(int type, double dtby4, double gama, do
     return r;
 }
 
-// solve_connector (src/spring.cpp:225-232): new bond from its RHS Gamma.
+// solve_connector (src/spring.cpp:174-181): new bond from its RHS Gamma.
 __device__ inline void solve_connector(const double g[3], double dt, const DevChain& c, double out[3], int& st) {
     const double gmag = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
     double r = implicit_length(c.spring_type, dt / 4.0, gmag / c.sqrtb, c.q0, st);
@@ -257,7 +257,7 @@ __device__ inline void solve_connector(const double g[3], double dt, const DevCh
     out[2] = s * g[2];
 }
 
-// Connector force factor at a bond of length len (src/spring.cpp:234-244).
+// Connector force factor at a bond of length len (src/spring.cpp:183-193).
 __device__ __forceinline__ double connector_factor(const DevChain& c, double len) {
     double r = len / c.sqrtb;
     if (fabs(r - 1.0) < kMyEps) r = 1.0 - kMyEps;
@@ -402,7 +402,7 @@ __device__ inline void bending_on_bead(const DevChain& c, int m, const double* u
 #undef U_
 }
 
-// RPY pair weights (src/hydrodynamics.cpp:77-98): omega1 (isotropic) and
+// RPY pair weights (src/hydrodynamics.cpp:36-43): omega1 (isotropic) and
 // omega2 (dyadic) for bead separation b with |b|^2 = sq (unclamped).
 __device__ __forceinline__ void rpy_weights(double hstar, double sq, double& om1, double& om2) {
     const double RPI = sqrt(kPi), TRPI = 2.0 * RPI, TPI = 2.0 * kPi;

@@ -147,7 +147,7 @@ __device__ __forceinline__ int sturm_count(const double* a, const double* b, int
     return count;
 }
 
-// The 100-step bisection of lanczos_extremes (src/hydrodynamics.cpp:251-260),
+// The 100-step bisection of lanczos_extremes (src/hydrodynamics.cpp:196-207),
 //   mid = 0.5*(lo+hi); if (sturm(mid) >= target) hi = mid; else lo = mid;
 // evaluated five levels at a time by one warp: lane l owns node l of a
 // depth-5 decision tree, replays the midpoints on its path with the same
@@ -270,7 +270,7 @@ struct Block {
     }
 
     // Matrix-free FP32 D.x: y_b = x_b + sum_{j != b} (om1 x_j + om2 (d.x_j) d),
-    // d = R_j - R_b, with omega from the RPY formula (src/hydrodynamics.cpp:77-105).
+    // d = R_j - R_b, with omega from the RPY formula (src/hydrodynamics.cpp:36-43).
     __device__ void apply_D_pairwise(const double* x, double* y) {
         for (int b = threadIdx.x; b < N; b += blockDim.x)
             vec32[b] = make_float4((float)x[3 * b], (float)x[3 * b + 1], (float)x[3 * b + 2], 0.f);
@@ -784,7 +784,7 @@ struct Block {
     }
 
     // Spring bead forces from bonds (connector_forces + bead_forces_from_connectors,
-    // src/spring.cpp:234-254). Fc: scratch for the bond forces.
+    // src/spring.cpp:183-207). Fc: scratch for the bond forces.
     __device__ void spring_from_geometry(const double* bond, const double* len, double* Fc, double* F) {
         for (int b = threadIdx.x; b < N - 1; b += blockDim.x) {
             const double f = connector_factor(ch, len[b]);
@@ -865,7 +865,7 @@ struct Block {
     }
 
     // Explicit force Fe = (EV + bending)(R) + external(t) (src/model.hpp:56-64,
-    // src/integrator.cpp:110-111). bond/len: geometry of R (already computed);
+    // src/integrator.cpp:75-76). bond/len: geometry of R (already computed);
     // u, cs: scratch.
     __device__ void explicit_force(const double* R, double t, const double* bond, const double* len, double* u,
                                    double* cs, double* out, bool with_external = true) {
@@ -956,7 +956,7 @@ struct Block {
             __syncthreads();
             return;
         }
-        // Gershgorin bracket (src/hydrodynamics.cpp:242-249)
+        // Gershgorin bracket (src/hydrodynamics.cpp:187-194)
         if (threadIdx.x == 0) {
             double lo = alpha[0], hi = alpha[0];
             for (int i = 0; i < k; ++i) {
@@ -1231,7 +1231,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 for (int b = tid; b < N; b += blockDim.x)
                     B.pos32[b] = make_float4((float)R[3 * b], (float)R[3 * b + 1], (float)R[3 * b + 2], 0.f);
             }
-            // Fs, Fe at R (src/integrator.cpp:105-111)
+            // Fs, Fe at R (src/integrator.cpp:70-76)
             B.geometry(R, Cv, E);
             __syncthreads();
             B.spring_from_geometry(Cv, E, F, Fs);
@@ -1345,7 +1345,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             B.explicit_force(Rp, t + dt, E, F, G, H, Cv);
             __syncthreads();
             if constexpr (kMixed) {
-                // D stays the tensor at R (built once per step, src/integrator.cpp:113)
+                // D stays the tensor at R (built once per step, src/integrator.cpp:78)
                 for (int b = tid; b < N; b += blockDim.x)
                     B.pos32[b] = make_float4((float)R[3 * b], (float)R[3 * b + 1], (float)R[3 * b + 2], 0.f);
                 __syncthreads();

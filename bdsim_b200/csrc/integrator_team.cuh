@@ -62,7 +62,7 @@ __device__ __forceinline__ int sturm_count_products(const double* a, const doubl
 }
 
 // Bisection for the target-th eigenvalue boundary on a half warp (16 lanes,
-// depth-4 speculative tree), the iteration of src/hydrodynamics.cpp:251-260.
+// depth-4 speculative tree), the iteration of src/hydrodynamics.cpp:196-207.
 static __device__ void halfwarp_bisect(const double* al, const double* bb, int k, int target, double& lo, double& hi) {
     const int lane = threadIdx.x & 15;
     const int lvl = 31 - __clz(lane + 1);
@@ -123,7 +123,7 @@ __device__ __forceinline__ int sturm_count_reg(const double (&a)[kLanczosWarm], 
 // Multisection for the target-th eigenvalue boundary on a half warp: 15 lanes
 // evaluate the Sturm count at 15 evenly spaced interior points of [lo, hi], a
 // ballot finds the sixteenth that holds the boundary (4 bits per round), the
-// iteration of src/hydrodynamics.cpp:251-260 in place of its halvings. Every
+// iteration of src/hydrodynamics.cpp:196-207 in place of its halvings. Every
 // lane of the half warp ends with the same lo, hi.
 static __device__ void halfwarp_multisect(const double (&a)[kLanczosWarm], const double (&b)[kLanczosWarm], int k,
                                           int target, double& lo, double& hi) {
@@ -351,7 +351,7 @@ struct TeamChain {
     }
 
     // ---- FP32 matrix-free D.x (Diffusion::apply, src/mobility.cpp:53-56;
-    // RPY weights src/hydrodynamics.cpp:77-105). x, y: the thread's two beads.
+    // RPY weights src/hydrodynamics.cpp:36-43). x, y: the thread's two beads.
     // K products against the same D in one pass over the bead pairs: the
     // pair geometry and weights are computed once for all K inputs (K = 3
     // for the products of a step that do not depend on one another).
@@ -690,7 +690,7 @@ struct TeamChain {
                 for (int d = 0; d < 3; ++d) vec[3 * bead(q) + d] = x[q][d];
     }
 
-    // Lanczos start vector (src/hydrodynamics.cpp:156-170): the normalised
+    // Lanczos start vector (src/hydrodynamics.cpp:152-155): the normalised
     // warm-start cache, or the normalised default seed when cold or when the
     // cache is zero.
     __device__ void start_vector(bool warm, const double* cache, double (&v)[2][3]) const {
@@ -1340,7 +1340,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             const double c8 = 0.125 * dt, c4 = 0.25 * dt;
             int lstat = 0;
             for (int iter = 0;; ++iter) {
-                // connector forces (src/spring.cpp:234-244) into s1, bead forces
+                // connector forces (src/spring.cpp:183-193) into s1, bead forces
                 double Fc[2][3];
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {

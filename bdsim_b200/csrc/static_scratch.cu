@@ -14,7 +14,9 @@
 //
 // Host code sees only a stand-in for the array's name; its device address is
 // taken once per device with cudaGetSymbolAddress (the first call on a device
-// does it; make that first call before any stream capture on the device).
+// does it, and the first call after the device's context was replaced, e.g.
+// by cudaDeviceReset; make that first call before any stream capture on the
+// device).
 // Every call shares the array and it keeps the last call's contents: the work
 // counters are cleared on each call, and everything else is written before it
 // is read. Calls that overlap on the GPU (two streams, two host threads) race
@@ -41,6 +43,8 @@ cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm);
 cudaError_t launch_mixed_team(int team_warps, const RunArgs& a, int grid, size_t smem, cudaStream_t s);
 cudaError_t occupancy_mixed_team(int team_warps, size_t smem, int* per_sm);
 DevChain derive_record(const bdcu_phys& p, const bdcu_sim& s, int64_t bead_off);
+int validate_chain(bdcu_ctx* ctx, int i, const bdcu_phys& p, const bdcu_sim& s, const double* arena,
+                   int64_t arena_len);
 }  // namespace bdcu
 
 using namespace bdcu;
@@ -53,15 +57,39 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_static_addr[kMaxDevices] = {};
+void* g_static_ctx[kMaxDevices] = {};
 
-// Device address of g_static_scratch on the current device (taken once).
+// The current CUDA context's handle (cuCtxGetCurrent, looked up through the
+// runtime so the library needs no link against the driver library); null if
+// unavailable.
+void* current_context() {
+    typedef int (*CtxGetCurrent)(void**);
+    static CtxGetCurrent fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrent>(p);
+    });
+    void* c = nullptr;
+    if (fn && fn(&c) != 0) c = nullptr;
+    return c;
+}
+
+// Device address of g_static_scratch on the current device. Taken at the first
+// call on a device, and again whenever the device's context has changed since
+// (after cudaDeviceReset the old address belongs to a destroyed context).
 cudaError_t static_base(int device, void** out) {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_static_addr[device]) {
+    void* cur = current_context();
+    if (!g_static_addr[device] || cur != g_static_ctx[device]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) return e;
         g_static_addr[device] = p;
+        g_static_ctx[device] = current_context();
     }
     *out = g_static_addr[device];
     return cudaSuccess;
@@ -88,28 +116,25 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
         return fail(ctx, BDCU_E_ARG, "bdcu_run_static: unknown form");
     if (arena_len < 0 || (arena_len > 0 && !arena)) return fail(ctx, BDCU_E_ARG, "bdcu_run_static: bad arena");
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, BDCU_E_ARG, "bdcu_run_static: bad device");
-    cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
 
-    // chain records, derived on the host exactly as bdcu_set_chains derives them
+    // chain records: the checks bdcu_set_chains makes (every table inside the
+    // arena), then the derivation bdcu_set_chains does -- all before the GPU
+    // is touched
     std::vector<DevChain> recs(n_chains);
     int64_t off = 0;
     int n_max = 0;
     for (int i = 0; i < n_chains; ++i) {
-        const bdcu_phys& p = phys[i];
-        if (p.n_beads < 2 || p.n_beads > kMaxBeads || !(sim[i].dt > 0.0))
-            return fail(ctx, BDCU_E_ARG, "bdcu_run_static: chain " + std::to_string(i) + " has bad n_beads or dt");
-        if (p.spring_type < 1 || p.spring_type > 7 || p.ev_type < 0 || p.ev_type > 4)
-            return fail(ctx, BDCU_E_ARG, "bdcu_run_static: chain " + std::to_string(i) + " has a bad spring/EV type");
-        const int64_t nn = (int64_t)p.n_beads * p.n_beads;
-        if ((p.phi_offset >= 0 && p.phi_offset + nn > arena_len) ||
-            (p.flow_n_times > 0 && p.flow_offset + 10 * (int64_t)p.flow_n_times > arena_len) ||
-            (p.ext_n_entries > 0 && p.ext_offset + 6 > arena_len))
-            return fail(ctx, BDCU_E_ARG, "bdcu_run_static: chain " + std::to_string(i) + " tables outside the arena");
-        recs[i] = derive_record(p, sim[i], off);
-        off += p.n_beads;
-        n_max = std::max(n_max, 3 * p.n_beads);
+        const int rc = validate_chain(ctx, i, phys[i], sim[i], arena, arena_len);
+        if (rc != BDCU_OK) {
+            ctx->err = "bdcu_run_static: " + ctx->err;
+            return rc;
+        }
+        recs[i] = derive_record(phys[i], sim[i], off);
+        off += phys[i].n_beads;
+        n_max = std::max(n_max, 3 * phys[i].n_beads);
     }
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return fail(ctx, BDCU_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     std::vector<double> seed(n_max);
     for (int i = 0; i < n_max; ++i) seed[i] = sin(0.7654321 * (i + 1)) + 0.5;
 

@@ -4,12 +4,12 @@ batch, advanced on the GPU chunk by chunk.
 
 Semantics kept from the reference:
   * trajectory i is seeded seed+i and starts from INITIALIZERS[method](N, seed+i)
-    (ensemble.py:197-199, 216-220);
+    (ensemble.py:157-161, 197-199);
   * a chunk of k steps is one integrate call over [t0, t0+(k-1)dt], and each
-    call starts the spectral (Lanczos) cache cold (ensemble.py:165-182);
+    call starts the spectral (Lanczos) cache cold (ensemble.py:106-123);
   * snapshots at step 0, every write_every steps and the last step;
   * a trajectory whose integration fails becomes a Failure, dropped and
-    reported, with MAX_FAILED_FRACTION enforced (ensemble.py:289-343).
+    reported, with MAX_FAILED_FRACTION enforced (ensemble.py:230, 244-284).
 """
 from __future__ import annotations
 
@@ -25,7 +25,7 @@ from .core import IntegratorError, integrate
 from .engine import Ensemble
 from .initial import (fene_fraenkel_bending_chain, fene_fraenkel_chain, fene_fraenkel_chain_aligned_x,
                       gaussian_chain)
-from .parallel import Failure
+from .failures import Failure
 from .params import PhysParams, Rng, SimParams
 
 
@@ -72,7 +72,7 @@ def _segment(sim: SimParams, t0: float, t1: float) -> SimParams:
 
 
 def n_steps_of(sim: SimParams) -> int:
-    """Integrator steps implied by sim's time span and dt (ensemble.py:154-156)."""
+    """Integrator steps implied by sim's time span and dt (ensemble.py:95-97)."""
     return int(round((sim.time_end - sim.time_start) / sim.dt))
 
 
@@ -131,7 +131,7 @@ def _start(phys, sim, n_traj, seed, initial, form, device):
 def simulate(phys: PhysParams, sim: SimParams, *, n_traj: int = 1, seed: int = 0, n_steps: int = None,
              initial: Initial = None, output: Output = None, backend: str = "cuda", n_workers: int = None,
              on_error: str = "skip", max_failed_fraction: float = None, form="plain", device: int = 0):
-    """Run n_traj chains on the GPU and write their snapshots (ensemble.py:238-277)."""
+    """Run n_traj chains on the GPU and write their snapshots (ensemble.py:179-227)."""
     _check_backend(backend)
     initial = initial or Initial()
     output = output or Output()
@@ -207,6 +207,29 @@ def sampled_states(R0, phys, sim, rng, sample_times):
     return [R for _t, R in trajectory_samples(R0, phys, sim, rng, sample_times)]
 
 
+# The reference's own reducers, by (module, name): run_ensemble batches these
+# when the reference's run layer hands them over with backend="cuda".
+_REFERENCE_REDUCERS = {
+    ("bdsim.ensemble", "final_state"): "final_state",
+    ("bdsim.ensemble", "sampled_states"): "sampled_states",
+    ("bdsim.rheology", "stress_series"): "stress_series",
+    ("bdsim.rheology", "viscosity_series"): "viscosity_series",
+    ("bdsim.rheology", "viscosity_series_vr"): "viscosity_series_vr",
+}
+
+
+def batched_reducer(fn):
+    """This package's batched equivalent of a per_trajectory reducer: the
+    function itself when it is one of ours, ours for the reference's
+    final_state / sampled_states / rheology series, else None."""
+    if fn is final_state or fn is sampled_states or fn in rheology.BATCHED:
+        return fn
+    name = _REFERENCE_REDUCERS.get((getattr(fn, "__module__", None), getattr(fn, "__qualname__", None)))
+    if name is None:
+        return None
+    return {"final_state": final_state, "sampled_states": sampled_states}.get(name) or getattr(rheology, name)
+
+
 def run_ensemble(phys: PhysParams, sim: SimParams, n_traj: int, per_trajectory, *, args=(), seed: int = 0,
                  initial: Initial = None, backend="cuda", n_workers=None, on_error="skip",
                  max_failed_fraction=None, form="plain", device: int = 0):
@@ -221,6 +244,7 @@ def run_ensemble(phys: PhysParams, sim: SimParams, n_traj: int, per_trajectory, 
     """
     _check_backend(backend)
     initial = initial or Initial()
+    per_trajectory = batched_reducer(per_trajectory) or per_trajectory
     if per_trajectory is final_state or per_trajectory is sampled_states:
         ens, _ = _start(phys, sim, n_traj, seed, initial, form, device)
         if per_trajectory is final_state:

@@ -176,10 +176,47 @@ class ExternalForce:
         return list(self._entries)
 
     def __getstate__(self):
-        return list(self._entries)
+        """Parallel arrays (beads, is_const, consts, times, ntimes, values), the
+        pickled layout of the reference's ExternalForce
+        (bindings/module.cpp:83-99)."""
+        beads, is_const, consts, times, ntimes, values = [], [], [], [], [], []
+        for bead, const, val, ts, vs in self._entries:
+            beads.append(int(bead))
+            is_const.append(1 if const else 0)
+            consts.extend(float(v) for v in val)
+            ntimes.append(len(ts))
+            times.extend(float(t) for t in ts)
+            for v in vs:
+                values.extend(float(x) for x in v)
+        return (beads, is_const, consts, times, ntimes, values)
 
     def __setstate__(self, s):
-        self._entries = [tuple(e) for e in s]
+        self._entries = list(external_entries(s))
+
+
+def external_entries(state):
+    """(bead, is_const, value(3), times, values) per entry, from an
+    ExternalForce state tuple in the reference's layout."""
+    beads, is_const, consts, times, ntimes, values = state
+    ti = vi = 0
+    for k, bead in enumerate(beads):
+        n = int(ntimes[k])
+        ts = tuple(float(t) for t in times[ti:ti + n])
+        vs = tuple(tuple(float(x) for x in values[vi + 3 * j:vi + 3 * j + 3]) for j in range(n))
+        ti += n
+        vi += 3 * n
+        yield (int(bead), bool(is_const[k]), tuple(float(x) for x in consts[3 * k:3 * k + 3]), ts, vs)
+
+
+def rng_state(rng):
+    """(ix, iy, seed) of an Rng: this package's or the reference's, whose only
+    accessor is its pickled state (bindings/module.cpp:302-303)."""
+    return tuple(int(v) for v in rng.__getstate__())
+
+
+def set_rng_state(rng, state):
+    """Write (ix, iy, seed) back into an Rng of either package."""
+    rng.__setstate__(tuple(int(v) for v in state))
 
 
 class PhysParams:

@@ -29,7 +29,7 @@ from . import properties as props
 from ._abi import CACHE_RESET_PER_CALL, ST_FATAL_MASK, count_steps
 from .core import IntegratorError, integrate, total_force
 from .engine import Ensemble
-from .parallel import Failure
+from .failures import Failure
 from .params import Flow, Rng
 
 # column of tau_xy in Ensemble.observables(): [Rg^2, tau_xx, tau_xy, ..., tau_zz]
@@ -59,7 +59,7 @@ def control_phys(phys):
     """The control chain's parameters: phys with a zero velocity gradient
     (rheology.py:92-93)."""
     phys_eq = copy.deepcopy(phys)
-    phys_eq.flow = Flow()
+    phys_eq.flow = type(phys.flow)()  # a default-constructed Flow is zero (either package's)
     return phys_eq
 
 

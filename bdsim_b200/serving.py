@@ -1,6 +1,6 @@
 """Serving: continuous batching of ensemble jobs on one GPU.
 
-bdsim runs one ensemble per `simulate` call (python/bdsim/ensemble.py:238-277).
+bdsim runs one ensemble per `simulate` call (python/bdsim/ensemble.py:179-227).
 A `Server` instead keeps a pool of chain slots resident on the device and
 admits jobs -- each the arguments of a `simulate` call -- while others run:
 
@@ -201,6 +201,12 @@ class Server:
         self.active_chains = 0
         self.chain_steps = 0
         self.t_first = None
+        # where the time goes: device time of the slice launches, slices run,
+        # chains selected per slice, counters of retired jobs' chains
+        self.device_ms = 0.0
+        self.n_slices = 0
+        self.selected_chains = 0
+        self.retired_counters = np.zeros(len(COUNTER_FIELDS), dtype=np.int64)
 
     # ------------------------------------------------------------------ API
 
@@ -263,19 +269,47 @@ class Server:
         return self.stats(t0)
 
     def stats(self, t0: float = None) -> dict:
+        """Latency and throughput of the jobs so far.
+
+        p50/p99_latency_s cover completed jobs (n_latency_samples of them).
+        Jobs still running or queued have waited at least now - arrival: with
+        those as censored samples, p50/p99_latency_lower_bound_s are lower
+        bounds of the percentiles over every admitted job
+        (n_admitted_samples). The breakdown says where the wall time went:
+        the share of it the GPU spent in slice launches, slices and chains per
+        slice, and corrector iterations and D.x products per chain-step."""
+        now = self.clock()
         lat = np.array([j.latency for j in self.done], dtype=np.float64)
         svc = np.array([j.t_done - j.t_admit for j in self.done], dtype=np.float64)
+        cens = np.array([now - j.t_arrival for j in self.running + self.queue], dtype=np.float64)
+        both = np.concatenate([lat, cens])
         t0 = self.t_first if t0 is None else t0
         # throughput over the whole replay: up to the last completion, or up
         # to now when nothing has completed yet
-        wall = ((max(j.t_done for j in self.done) if self.done else self.clock()) - t0) if t0 is not None else 0.0
+        wall = ((max(j.t_done for j in self.done) if self.done else now) - t0) if t0 is not None else 0.0
+        span = (now - t0) if t0 is not None else 0.0
         pct = (lambda a, q: float(np.percentile(a, q)) if a.size else None)
+        cnt = self.retired_counters.copy()
+        if self.running:  # retired jobs' rows were zeroed when they left: the pool holds running jobs only
+            cnt = cnt + self.counters.sum(dim=0).cpu().numpy().astype(np.int64)
+        c = dict(zip(COUNTER_FIELDS, (int(v) for v in cnt)))
+        steps = max(c["steps"], 1)
         return {"jobs_completed": len(self.done), "jobs_rejected": len(self.rejected),
                 "jobs_queued": len(self.queue), "jobs_running": len(self.running),
-                "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+                "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99), "n_latency_samples": int(lat.size),
+                "p50_latency_lower_bound_s": pct(both, 50), "p99_latency_lower_bound_s": pct(both, 99),
+                "n_admitted_samples": int(both.size),
                 "p50_service_s": pct(svc, 50), "p99_service_s": pct(svc, 99),
                 "chain_steps": int(self.chain_steps), "wall_s": wall,
-                "chain_steps_per_s": (self.chain_steps / wall) if wall > 0 else None}
+                "chain_steps_per_s": (self.chain_steps / wall) if wall > 0 else None,
+                "breakdown": {
+                    "gpu_busy_frac": (self.device_ms * 1e-3 / span) if span > 0 else None,
+                    "slices": self.n_slices,
+                    "chains_per_slice": (self.selected_chains / self.n_slices) if self.n_slices else None,
+                    "corrector_iters_per_step": c["corrector_iters"] / steps,
+                    "dx_per_step": c["dx_products"] / steps,
+                    "nonconverged_step_frac": c["nonconverged"] / steps,
+                    "chain_steps_per_device_s": (self.chain_steps / (self.device_ms * 1e-3)) if self.device_ms else None}}
 
     # ------------------------------------------------------------ internals
 
@@ -363,8 +397,15 @@ class Server:
         if key != self._selected:
             self.ctx.select(sel)
             self._selected = key
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record()
         self.ctx.run_slice(self.R, self.rng, self.cache, self.valid, self.t0, self.k, self.status, self.counters,
                            self.form, CACHE_PERSIST, self.budget_ns, self.steps_done, self.t_end)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e1.record()
+        self._slice_events = (e0, e1)
+        self.n_slices += 1
+        self.selected_chains += len(sel)
         self.done_host[:hi_slot].copy_(self.steps_done[:hi_slot], non_blocking=True)
         self.tend_host[:hi_slot].copy_(self.t_end[:hi_slot], non_blocking=True)
         self.status_host[:hi_slot].copy_(self.status[:hi_slot], non_blocking=True)
@@ -375,6 +416,8 @@ class Server:
     def _finish_slice(self, work, sel, ev=None):
         if ev is not None:
             ev.synchronize()
+            e0, e1 = self._slice_events
+            self.device_ms += e0.elapsed_time(e1)
         sel = np.asarray(sel, dtype=np.int64)
         if sel.size:
             done = self.done_host.numpy()[sel]
@@ -408,6 +451,10 @@ class Server:
 
     def _retire(self, js: JobState):
         n = int(js.job.n_traj)
+        rows = self.counters[js.slot0:js.slot0 + n].sum(dim=0).cpu().numpy()
+        js.counters = dict(zip(COUNTER_FIELDS, (int(v) for v in rows)))
+        self.retired_counters += rows.astype(np.int64)
+        self.counters[js.slot0:js.slot0 + n].zero_()
         self.running.remove(js)
         self.done.append(js)
         self.slots.free(js.slot0, n)

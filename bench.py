@@ -43,7 +43,10 @@ CHUNK = 100
 DT = 1e-3
 WORKLOAD = ("4096 chains x N=50, FENE b=50, RPY h*=0.25 Chebyshev+Lanczos, Gauss EV z*=1 d*=0.5, "
             "shear 1.0, dt=1e-3, gaussian_chain(50, bond_std=1, seed=i), Rng(i)")
+WORKLOAD_SHORT = "4096 x N=50 FENE b=50, RPY h*=0.25 Chebyshev, Gauss EV, shear 1, dt=1e-3 (cfg2)"
 METRIC = "chain-steps/sec at N=50 HI (FP32-mixed vs FP64 plain, 1 B200)"
+# the lighter serving stream: the same job mix, shorter jobs, fewer arrivals
+LIGHT = {"scale_steps": 0.01, "rate": 2.0, "horizon": 20.0}
 SERVING_WORKLOAD = ("Poisson arrivals 200 jobs/s; N ~ U{10..300}, n_traj ~ U{1..256}, n_steps log-uniform "
                     "[1e3, 1e5], shear or uniaxial at U[0.1, 5], FENE b=100, h*=0.25 Chebyshev, write_every=100; "
                     "replayed in real time for the horizon; shortest-job-first admission under a 256-job queue "
@@ -137,17 +140,18 @@ def flush_l2(torch, buf):
 
 def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, bounds_every=1):
     """Warm up, then time `steps` chunks with CUDA events on the launch stream.
-    bounds_every: the mixed form's spectral-bound refresh interval (1: every
-    step, the reference's policy)."""
+    Each chunk starts its spectral (Lanczos) cache cold, as each integrate call
+    of the reference's chunked simulate does. bounds_every: the mixed form's
+    spectral-bound refresh interval (1: every step, the reference's policy)."""
     import bdsim_b200 as B
-    from bdsim_b200._abi import CACHE_PERSIST
+    from bdsim_b200._abi import CACHE_RESET_PER_CALL
     n = len(Rs)
     with torch.cuda.stream(stream):
         ens = B.Ensemble([phys] * n, [sim] * n, Rs, [(1, -1, rank_seed0 + i) for i in range(n)], form=form)
         ens.ctx.set_bounds_refresh(bounds_every)
         t = 0.0
         for _ in range(warmup):
-            ens.advance(t, CHUNK, CACHE_PERSIST)
+            ens.advance(t, CHUNK, CACHE_RESET_PER_CALL)
             t += CHUNK * DT
         stream.synchronize()
         c0 = ens.counter_totals()
@@ -158,7 +162,7 @@ def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, boun
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            ens.advance(t, CHUNK, CACHE_PERSIST)
+            ens.advance(t, CHUNK, CACHE_RESET_PER_CALL)
             e1.record(stream)
             t += CHUNK * DT
             e1.synchronize()
@@ -356,6 +360,7 @@ def cpu_reference(seconds_target=15.0, threads=None):
     _, _, status = orc.integrate_many(Rs, [phys] * chains, [s] * chains, [(1, -1, i) for i in range(chains)], threads)
     wall = time.perf_counter() - t0
     return {"value": chains * steps / wall, "unit": "chain-steps/s", "cores": threads, "kind": kind,
+            "wall_s": wall,
             "sample": f"{chains} of the {N_CHAINS} chains x {steps} steps (one chunk, cold Lanczos start), "
                       f"{threads} threads, {wall:.1f} s wall"}
 
@@ -401,18 +406,23 @@ def main():
         if rank != 0:
             return 0
         steps, warmup = args.steps, args.warmup
-        vals = []
+        vals, walls = [], []
         base = None
         for i in range(warmup + steps):
-            r = cpu_reference(seconds_target=8.0)
+            r = cpu_reference(seconds_target=10.0)
             if i >= warmup:
                 vals.append(r["value"])
+                walls.append(r["wall_s"])
                 base = r
         v = float(np.median(vals))
+        # a step of this arm is one bounded sample of the workload (a subset of
+        # the chains for one 100-step chunk); ms_per_step is its measured wall time
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "chain-steps/s", "n_gpus": args.gpus,
-                "steps": steps, "warmup": warmup, "ms_per_step": N_CHAINS * CHUNK / v * 1e3,
+                "steps": steps, "warmup": warmup, "ms_per_step": float(np.median(walls)) * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": WORKLOAD, "chunk_steps": CHUNK, "n_chains": N_CHAINS},
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD_SHORT, "chunk_steps": CHUNK, "n_chains_per_gpu": N_CHAINS,
+                           "step": base["sample"]},
                 "cpu_baseline": {"value": v, "unit": "chain-steps/s", "cores": base["cores"], "kind": base["kind"],
                                  "sample": base["sample"]},
                 "e2e": {"value": v, "unit": "chain-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -469,9 +479,13 @@ def main():
         r["total_ms"] = reduce_max(sum(r["ms"]), dist, device="cuda")
         results["mixed_k4"] = r
     e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), max(3, args.warmup), first, "mixed")
-    serving = None
+    serving = light = None
     if args.serving_seconds > 0 and set(forms) == {"plain", "mixed"}:
+        # the serving configuration as stated (overload), then a lighter stream
+        # of the same job mix that one GPU serves to completion
         serving = run_serving(torch, args.serving_seconds, seed=rank)
+        light = run_serving(torch, LIGHT["horizon"], scale_steps=LIGHT["scale_steps"], rate=LIGHT["rate"],
+                            seed=rank + 1, drain=True)
 
     if rank != 0:
         if dist is not None:
@@ -510,6 +524,37 @@ def main():
             cpu = cpu_reference()
         except Exception as exc:  # reported, not fatal
             cpu = {"error": str(exc)}
+    ens_m = compare_observables(mixed["obs"], plain["obs"])
+    ens_k4 = compare_observables(results["mixed_k4"]["obs"], plain["obs"])
+    # detail lines first; the headline line (last, compact) repeats the key figures
+    print(json.dumps({"detail": "ensemble_mixed_vs_plain", **ens_m,
+                      "steps_per_chain": (args.warmup + args.steps) * CHUNK, "n_chains": n_chains,
+                      "note": "final state of each form from the same initial chains and seeds"}))
+    print(json.dumps({"detail": "mixed_bounds_every_4", "value": rate(results["mixed_k4"]), "unit": "chain-steps/s",
+                      "dx_per_step": flops_per_chain_step(results["mixed_k4"]["counters"])[1],
+                      "ensemble_vs_plain": ens_k4,
+                      "policy": "spectral bounds kept for 4 steps, refreshed early when a step's Chebyshev check "
+                                "fails on them (bdcu_set_bounds_refresh; not the reference's policy)"}))
+    print(json.dumps({"detail": "roofline", "flops_per_chain_step": fl_p, "dx_per_step_algorithm": dx_p,
+                      "dx_per_step_mixed": dx_m, "fp32_fma_peak_tflops": peak32, "fp64_fma_peak_tflops": peak64,
+                      "plain_tflops_dense_equiv": achieved_p, "plain_frac_of_fp64_peak": achieved_p / peak64,
+                      "hbm_peak_gbs_measured": _peaks().get("hbm_gbs"),
+                      "peak_source": "FMA-loop kernels (libbdsim_peak.so) timed in this run; the integrator runs "
+                                     "on CUDA cores, neither HBM- nor tensor-bound"}))
+    for name, st in (("serving_overload", serving), ("serving_light", light)):
+        if st is not None:
+            print(json.dumps({"detail": name, **st}))
+    print(json.dumps({"detail": "serving_workload", "overload": SERVING_WORKLOAD,
+                      "light": f"the same job mix with n_steps x{LIGHT['scale_steps']} (min 100), "
+                               f"{LIGHT['rate']} jobs/s for {LIGHT['horizon']} s, drained"}))
+
+    def lat(st):
+        if st is None:
+            return None
+        return {"p50_s": _r(st["p50_latency_s"]), "p99_s": _r(st["p99_latency_s"]), "n": st["n_latency_samples"],
+                "p50_lb_s": _r(st["p50_latency_lower_bound_s"]), "p99_lb_s": _r(st["p99_latency_lower_bound_s"]),
+                "n_all": st["n_admitted_samples"], "chain_steps_per_s": _r(st["chain_steps_per_s"])}
+
     line = {
         "metric": METRIC,
         "value": rate(mixed),
@@ -523,48 +568,32 @@ def main():
         "vs_baseline": None,
         "dtype": "f32+f64 (mixed)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "mixed", "chunk_steps": CHUNK, "n_chains_per_gpu": n_chains,
-                   "n_beads": N_BEADS, "l2": "flushed (256 MiB write) between timed chunks",
-                   "parallelism": f"trajectory shards x{world}"},
-        "plain_fp64": {"value": rate(plain), "unit": "chain-steps/s", "ms_per_step": plain["total_ms"] / args.steps,
-                       "dx_per_step": dx_p, "tflops_dense_equiv": achieved_p,
-                       "fp64_frac_of_measured_fma_peak": achieved_p / peak64},
+        "plain_fp64": {"value": rate(plain), "ms_per_step": plain["total_ms"] / args.steps},
         "mixed_over_plain": rate(mixed) / rate(plain),
+        "config": {"workload": WORKLOAD_SHORT, "form": "mixed", "chunk_steps": CHUNK, "n_chains_per_gpu": n_chains,
+                   "cache": "cold per chunk", "l2": "flushed (256 MiB write) between timed chunks",
+                   "parallelism": f"trajectory shards x{world}", "plain_fp64_value": rate(plain),
+                   "mixed_over_plain": rate(mixed) / rate(plain)},
         "roofline": {"bound": "fp32-simt", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
-                     "frac": achieved / peak32, "traffic": traffic,
-                     "peak_source": "measured in this run: FP32 FMA-loop kernel (libbdsim_peak.so); the kernel "
-                                    "runs on CUDA cores, neither HBM- nor tensor-bound",
-                     "flops_per_chain_step": fl_p, "dx_per_step_algorithm": dx_p, "dx_per_step_mixed": dx_m,
-                     "hbm_peak_gbs_measured": _peaks().get("hbm_gbs")},
+                     "frac": achieved / peak32, "traffic": traffic},
         "e2e": None if e2e is None else {
-            "value": e2e[0], "unit": "chain-steps/s", "h2d_bytes_per_step": e2e[1], "d2h_bytes_per_step": e2e[2],
-            "path": "bdcu_integrate_host, pinned host R/RNG, cold spectral cache per call"},
+            "value": e2e[0], "unit": "chain-steps/s", "h2d_bytes_per_step": e2e[1], "d2h_bytes_per_step": e2e[2]},
         "gpu_launches": args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
         "failed_chains": {"mixed": mixed["failed"], "plain": plain["failed"]},
-        "mixed_bounds_every_4": {
-            "value": rate(results["mixed_k4"]), "unit": "chain-steps/s",
-            "dx_per_step": flops_per_chain_step(results["mixed_k4"]["counters"])[1],
-            "ensemble_vs_plain": compare_observables(results["mixed_k4"]["obs"], plain["obs"]),
-            "policy": "FP32-mixed form with the spectral bounds kept for 4 steps and refreshed early when a "
-                      "step's Chebyshev check fails on them (bdcu_set_bounds_refresh; not the reference's policy, "
-                      "so not the headline)"},
-        "ensemble": dict(compare_observables(mixed["obs"], plain["obs"]),
-                         steps_per_chain=(args.warmup + args.steps) * CHUNK, n_chains=n_chains,
-                         note="final state of each form from the same initial chains and seeds"),
-        "latency": None if serving is None else {
-            "p50_s": serving["p50_latency_s"], "p99_s": serving["p99_latency_s"],
-            "workload": SERVING_WORKLOAD, "under": "overload (offered load far above one GPU's capacity)",
-            **{k: serving[k] for k in ("jobs_offered", "jobs_completed", "jobs_rejected", "jobs_running",
-                                       "jobs_queued", "horizon_s", "chain_steps_per_s", "p50_service_s",
-                                       "p99_service_s", "queue_limit", "max_active_chains", "policy",
-                                       "slice_steps", "slice_budget_s")}},
+        "ensemble_sigma": {"rg2": _r(ens_m["rg2"]["diff_in_sigma"]), "tau_xy": _r(ens_m["tau_xy"]["diff_in_sigma"])},
+        "latency": {"overload": lat(serving), "light": lat(light)},
     }
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def _r(v, digits=4):
+    """v to `digits` significant digits (None stays None)."""
+    return None if v is None else float(f"{v:.{digits}g}")
 
 
 def _peaks():

@@ -11,12 +11,12 @@
  *
  *   bdcu_integrate_host   _bdsim.integrate(R, phys, sim, rng)
  *                         bindings/module.cpp:45-50  ->  time_integrate_chain
- *                         src/integrator.hpp:32, src/integrator.cpp:209-212
+ *                         src/integrator.hpp:32, src/integrator.cpp:174-177
  *                         (batched: many chains, one call; the RNG state and
  *                         R are updated in place exactly as the reference
  *                         mutates its Rng and returns the evolved R)
  *   bdcu_run              the same step loop on device-resident state
- *                         (ChainIntegrator::run, src/integrator.cpp:101-120)
+ *                         (ChainIntegrator::run, src/integrator.cpp:66-85)
  *   bdcu_total_force      _bdsim.total_force(R, phys)
  *                         bindings/module.cpp:67-76
  *   bdcu_forces           _bdsim.spring_force / ev_force / bending_force /
@@ -74,7 +74,7 @@ enum {
 /* ---- spectral-cache policy across calls ---- */
 enum {
     /* the reference: each integrate call starts Lanczos cold
-       (src/integrator.cpp:211 builds a fresh PhysicalModel per call) */
+       (src/integrator.cpp:176 builds a fresh PhysicalModel per call) */
     BDCU_CACHE_RESET_PER_CALL = 0,
     /* keep the warm-start vector across calls (a chunked run then equals one
        continuous call of the reference) */
@@ -84,7 +84,7 @@ enum {
 /* ---- per-chain status bits (device word per chain) ---- */
 enum {
     BDCU_ST_NONCONVERGED = 1,  /* corrector hit 100N iterations; step accepted
-                                  (src/integrator.cpp:195-198) */
+                                  (src/integrator.cpp:160-163) */
     BDCU_ST_NOT_PD = 2,        /* Cholesky pivot <= 0; chain stopped
                                   (src/linalg.cpp:16-25,99) */
     BDCU_ST_CHEB_FALLBACK = 4, /* Chebyshev FD check failed, Cholesky used
@@ -139,7 +139,7 @@ typedef struct bdcu_phys {
 } bdcu_phys;
 
 /* SimParams (src/integrator.hpp:22-28). time_start/time_end bound the step
-   loop exactly as ChainIntegrator::run does (src/integrator.cpp:102). */
+   loop exactly as ChainIntegrator::run does (src/integrator.cpp:67). */
 typedef struct bdcu_sim {
     double time_start;
     double time_end;
@@ -151,7 +151,7 @@ typedef struct bdcu_sim {
 
 /* Per-chain counters (device). They replace the reference's only in-code
    counters, SpectralCache::cold_runs/warm_runs (src/hydrodynamics.hpp:33-37),
-   and its global nonconvergence_count (src/integrator.cpp:60). */
+   and its global nonconvergence_count (src/integrator.cpp:25). */
 typedef struct bdcu_counters {
     int64_t steps;            /* integrator steps completed */
     int64_t dx_products;      /* D.x products (the dominant work unit) */
@@ -217,7 +217,7 @@ int bdcu_run(bdcu_ctx* ctx, double* R, int32_t* rng, double* cache,
 
 /* bdcu_run with a time slice, for serving loops that share the GPU between
    jobs (no counterpart in the reference, whose integrate calls run to
-   completion, ChainIntegrator::run, src/integrator.cpp:101-120): a chain
+   completion, ChainIntegrator::run, src/integrator.cpp:66-85): a chain
    starts no new step once budget_ns nanoseconds have passed since its thread
    block started (0: no limit; a step in progress always completes), so one
    slow chain (e.g. a corrector at its 100N-iteration cap) cannot hold the
@@ -327,6 +327,15 @@ int bdcu_write_arena(bdcu_ctx* ctx, int64_t offset, const double* values, int64_
    selects every chain (not allowed for a pool). */
 int bdcu_select(bdcu_ctx* ctx, int count, const int32_t* slots);
 
+/* The checks bdcu_set_chains, bdcu_update_chains and bdcu_run_static make on
+   chain records (bead count, dt, spring/EV types, every flow, phi and
+   external-force table inside the arena), without a GPU or a context. No
+   counterpart in the reference, whose constructors trust their inputs. Returns
+   the first failing chain's status and copies its message into msg (msg_len
+   bytes including the terminator; msg may be NULL). */
+int bdcu_check_chains(int n_chains, const bdcu_phys* phys, const bdcu_sim* sim, const double* arena,
+                      int64_t arena_len, char* msg, int msg_len);
+
 /* bdcu_run for callers that cannot allocate device memory. No counterpart in
    the reference: bdsim runs on the CPU and never allocates GPU memory.
    Some callers cannot call cudaMalloc -- a host application whose memory pool
@@ -340,11 +349,16 @@ int bdcu_select(bdcu_ctx* ctx, int count, const int32_t* slots);
    the library holds until process exit. It calls no cudaMalloc/cudaFree.
    ctx comes from bdcu_create (which allocates no device memory) and supplies
    the device, the stream and bdcu_last_error; bdcu_set_chains is not used.
+   - Chain records get the checks of bdcu_set_chains (bdcu_check_chains)
+     before the GPU is touched: a table outside the arena is BDCU_E_ARG, a
+     chain beyond the bead limit BDCU_E_LIMIT.
    - Batches whose parameters plus one block's scratch exceed the array return
      BDCU_E_LIMIT with a message; smaller batches run with as many concurrent
      blocks as fit (fewer than bdcu_run may use).
    - The first call on a device takes the array's device address
-     (cudaGetSymbolAddress): make it before any stream capture on that device.
+     (cudaGetSymbolAddress), and so does the first call after the device's
+     context was replaced (cudaDeviceReset): make that call before any stream
+     capture on that device.
    - Every call shares the array and leaves its contents behind; the work
      counters are cleared by each call. Calls that overlap on the GPU race on the
      array: serialise them. */

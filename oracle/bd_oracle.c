@@ -19,8 +19,8 @@
 #define PI_D 3.14159265358979323846 /* src/types.hpp:22 */
 #define MYEPS_D 1e-6                /* src/types.hpp:24 */
 #define MAXCHEB_I 500               /* src/types.hpp:20 */
-#define LANCZOS_COLD_I 30           /* src/hydrodynamics.cpp:134 */
-#define LANCZOS_WARM_I 8            /* src/hydrodynamics.cpp:135 */
+#define LANCZOS_COLD_I 30           /* src/hydrodynamics.cpp:79 */
+#define LANCZOS_WARM_I 8            /* src/hydrodynamics.cpp:80 */
 
 /* std::min / std::max semantics, NaN behaviour included. */
 static double mind(double a, double b) { return (b < a) ? b : a; }
@@ -347,7 +347,7 @@ int bdo_solve_connector(const double gamma[3], double dt, const bdcu_phys* p, do
     return st;
 }
 
-/* connector_forces (src/spring.cpp:234-244) from bonds/lengths. */
+/* connector_forces (src/spring.cpp:183-193) from bonds/lengths. */
 static void connector_forces(const double* bond, const double* len, int nb, const bdcu_phys* p, double* Fb) {
     const double sqrtb = p->sqrtb;
     const double q0 = p->natural_length / sqrtb;
@@ -359,7 +359,7 @@ static void connector_forces(const double* bond, const double* len, int nb, cons
     }
 }
 
-/* bead_forces_from_connectors (src/spring.cpp:246-254) */
+/* bead_forces_from_connectors (src/spring.cpp:195-203) */
 static void bead_forces(const double* Fb, int N, double* F) {
     memset(F, 0, sizeof(double) * 3 * (size_t)N);
     if (N == 1) return;
@@ -931,7 +931,7 @@ static void apply_D(chain_ws* w, const double* x, double* y, bdcu_counters* cnt)
     if (cnt) cnt->dx_products++;
 }
 
-/* Fe = (EV + bending)(R) + external(t) (src/model.hpp:56-64, integrator.cpp:110-111). */
+/* Fe = (EV + bending)(R) + external(t) (src/model.hpp:56-64, src/integrator.cpp:75-76). */
 static void explicit_force(chain_ws* w, const double* R, double t, double* Fe) {
     const int N = w->N;
     double* a = (double*)malloc(sizeof(double) * 3 * (size_t)N);
@@ -991,7 +991,7 @@ int bdo_integrate(double* R, const bdcu_phys* p, const bdcu_sim* s, const double
             for (int i = 0; i < N; ++i)
                 for (int d = 0; d < 3; ++d) R[3 * i + d] = R[3 * i + d] - com[d];
         }
-        /* Fs, Fe (src/integrator.cpp:105-111) */
+        /* Fs, Fe (src/integrator.cpp:70-76) */
         bdo_spring_force(R, N, p, Fs);
         explicit_force(&w, R, t, Fe);
         /* D (src/mobility.cpp:39-51) */

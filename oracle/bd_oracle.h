@@ -25,12 +25,12 @@ extern "C" {
 /* Rng::ran_1 (src/rng.cpp:41-70) on state {ix, iy, seed}. */
 void bdo_ran1(int32_t state[3], int n, double* out);
 
-/* solve_implicit_r (src/spring.cpp:174-223): reduced length and force factor.
+/* solve_implicit_r (src/spring.cpp:123-172): reduced length and force factor.
    Returns 0, or a BDCU_ST_* bit on failure. */
 int bdo_solve_implicit_r(int spring_type, double dtby4, double gama, double natscl,
                          double* length, double* force_factor);
 
-/* solve_connector (src/spring.cpp:225-232). */
+/* solve_connector (src/spring.cpp:174-181). */
 int bdo_solve_connector(const double gamma[3], double dt, const bdcu_phys* p, double out[3]);
 
 /* Per-bead forces at R (N x 3 row-major). arena: see bdsim_cuda.h. */
@@ -58,7 +58,7 @@ void bdo_chebyshev_sqrt_times(const double* D, int n, const double* x0, double m
                               double fd_tol, double* cache_vec, int* cache_valid,
                               double* out, int* nterms, double* fd_err);
 
-/* time_integrate_chain (src/integrator.cpp:209-212): integrate R (N x 3) in
+/* time_integrate_chain (src/integrator.cpp:174-177): integrate R (N x 3) in
    place over sim's [time_start, time_end]. rng advanced in place.
    cache_vec/cache_valid: if NULL a fresh cache is used (the reference's
    per-call reset); else the given cache persists across calls.

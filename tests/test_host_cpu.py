@@ -136,3 +136,56 @@ def test_no_cpu_fallback_without_gpu():
         pytest.skip("a GPU is visible")
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         B.integrate(np.zeros((4, 3)), PhysParams(), SimParams(), Rng(1))
+
+
+def _external_case_records():
+    from tests.golden.cases import build_case
+    R0, phys, sim, _ = build_case("ilc_timeflow_external")
+    prec, srec, arena = _abi.pack_batch([phys], [sim], [len(R0)])
+    assert prec[0].ext_n_entries >= 2
+    return prec, srec, arena
+
+
+def test_check_chains_accepts_a_valid_record():
+    prec, srec, arena = _external_case_records()
+    rc, msg = _abi.check_records(1, prec, srec, arena)
+    assert rc == 0, msg
+
+
+def test_check_chains_rejects_a_negative_external_offset():
+    """bdcu_run_static and bdcu_set_chains share these checks; a record that
+    points before the arena never reaches a kernel."""
+    prec, srec, arena = _external_case_records()
+    prec[0].ext_offset = -1
+    rc, msg = _abi.check_records(1, prec, srec, arena)
+    assert rc == 1 and "external force list outside the arena" in msg
+
+
+def test_check_chains_rejects_an_external_table_past_the_arena():
+    prec, srec, arena = _external_case_records()
+    # the second entry's sample count (header word 5) runs past the arena's end
+    first = int(prec[0].ext_offset)
+    nt0 = int(arena[first + 5])
+    second = first + 6 + 4 * nt0
+    bad = arena.copy()
+    bad[second + 5] = float(arena.size)
+    rc, msg = _abi.check_records(1, prec, srec, bad)
+    assert rc == 1 and "external force list outside the arena" in msg
+    # and a list whose entry count walks off the end
+    prec[0].ext_n_entries = 1000
+    rc, msg = _abi.check_records(1, prec, srec, arena)
+    assert rc == 1
+
+
+def test_check_chains_rejects_negative_flow_offset_and_bead_limit():
+    from tests.golden.cases import build_case
+    R0, phys, sim, _ = build_case("ilc_timeflow_external")
+    prec, srec, arena = _abi.pack_batch([phys], [sim], [len(R0)])
+    if prec[0].flow_n_times > 0:
+        prec[0].flow_offset = -5
+        rc, msg = _abi.check_records(1, prec, srec, arena)
+        assert rc == 1 and "flow table" in msg
+    prec, srec, arena = _abi.pack_batch([phys], [sim], [len(R0)])
+    prec[0].n_beads = 5000
+    rc, msg = _abi.check_records(1, prec, srec, arena)
+    assert rc == 5 and "n_beads" in msg

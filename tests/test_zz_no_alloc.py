@@ -64,6 +64,8 @@ def test_static_entry_point_matches_bdcu_run_twice(form):
         t0 = torch.tensor(t, dtype=torch.float64, device=dev)
         k = torch.tensor(steps, dtype=torch.int32, device=dev)
         ens.advance(t, steps, _abi.CACHE_PERSIST)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(0)[0]
         rc = lib.bdcu_run_static(ctx.h, n, prec, srec, arena.ctypes.data_as(_abi.c_double_p), arena.size,
                                  _abi.dptr(R), _abi.dptr(rng), _abi.dptr(cache), _abi.dptr(valid), _abi.dptr(t0),
                                  _abi.dptr(k), _abi.dptr(status), _abi.dptr(counters),
@@ -71,6 +73,10 @@ def test_static_entry_point_matches_bdcu_run_twice(form):
                                  _abi.CACHE_PERSIST)
         assert rc == 0, lib.bdcu_last_error(ctx.h).decode()
         torch.cuda.synchronize()
+        if call == 1:
+            # the first call loads the module and takes the array's address;
+            # the second must leave the device's free memory as it found it
+            assert torch.cuda.mem_get_info(0)[0] == free_before
         want = ens.R.cpu().numpy()
         got = R.cpu().numpy()
         assert np.array_equal(ens.status.cpu().numpy(), status.cpu().numpy()), call
@@ -101,3 +107,30 @@ def test_static_entry_point_rejects_a_batch_beyond_its_maximum():
                                  _abi.dptr(z1), _abi.dptr(z1), _abi.dptr(cnt), 0, _abi.CACHE_RESET_PER_CALL)
     assert rc == 5  # BDCU_E_LIMIT
     assert "maximum" in ctx.lib.bdcu_last_error(ctx.h).decode()
+
+
+def test_static_entry_point_rejects_a_record_outside_the_arena():
+    """The record checks of bdcu_set_chains apply before anything is launched:
+    an external-force list that starts before the arena is BDCU_E_ARG."""
+    import torch
+    R0, p, s, seed = build_case("ilc_timeflow_external")
+    prec, srec, arena = _abi.pack_batch([p], [s], [len(R0)])
+    prec[0].ext_offset = -1
+    ctx = B.Context(0)
+    dev = torch.device("cuda", 0)
+    n = len(R0)
+    R = torch.from_numpy(R0).to(dev)
+    rng = torch.tensor([[1, -1, seed]], dtype=torch.int32, device=dev)
+    zc = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    z1 = torch.zeros(1, dtype=torch.int32, device=dev)
+    t0 = torch.zeros(1, dtype=torch.float64, device=dev)
+    k = torch.ones(1, dtype=torch.int32, device=dev)
+    cnt = torch.zeros((1, 8), dtype=torch.int64, device=dev)
+    before = R.clone()
+    rc = ctx.lib.bdcu_run_static(ctx.h, 1, prec, srec, arena.ctypes.data_as(_abi.c_double_p), arena.size,
+                                 _abi.dptr(R), _abi.dptr(rng), _abi.dptr(zc), _abi.dptr(z1), _abi.dptr(t0),
+                                 _abi.dptr(k), _abi.dptr(z1), _abi.dptr(cnt), 0, _abi.CACHE_RESET_PER_CALL)
+    torch.cuda.synchronize()
+    assert rc == 1  # BDCU_E_ARG
+    assert "outside the arena" in ctx.lib.bdcu_last_error(ctx.h).decode()
+    assert torch.equal(R, before)
