@@ -245,10 +245,12 @@ class Server:
             self.step()
             it += 1
 
-    def run_stream(self, jobs, arrivals, horizon: float = None, drain: bool = True):
+    def run_stream(self, jobs, arrivals, horizon: float = None, drain: bool = True, drain_limit: float = None):
         """Replay an arrival stream in real time: jobs[i] arrives arrivals[i]
         seconds after the start. Stops admitting at `horizon` seconds (if
-        given) and, with drain, runs the admitted work to completion."""
+        given) and, with drain, runs the admitted work to completion, or for
+        at most `drain_limit` seconds past the horizon (jobs still running
+        then are reported as censored)."""
         order = np.argsort(arrivals, kind="stable")
         t0 = self.clock()
         i = 0
@@ -263,7 +265,8 @@ class Server:
                     break
                 time.sleep(max(0.0, min(0.05, arrivals[order[i]] - now)))
                 continue
-            if horizon is not None and now > horizon and not drain:
+            if horizon is not None and now > horizon and (not drain or
+                                                         (drain_limit is not None and now > horizon + drain_limit)):
                 break
             self.step()
         return self.stats(t0)

@@ -46,7 +46,7 @@ WORKLOAD = ("4096 chains x N=50, FENE b=50, RPY h*=0.25 Chebyshev+Lanczos, Gauss
 WORKLOAD_SHORT = "4096 x N=50 FENE b=50, RPY h*=0.25 Chebyshev, Gauss EV, shear 1, dt=1e-3 (cfg2)"
 METRIC = "chain-steps/sec at N=50 HI (FP32-mixed vs FP64 plain, 1 B200)"
 # the lighter serving stream: the same job mix, shorter jobs, fewer arrivals
-LIGHT = {"scale_steps": 0.01, "rate": 2.0, "horizon": 20.0}
+LIGHT = {"scale_steps": 0.01, "rate": 2.0, "horizon": 20.0, "drain_limit": 20.0}
 SERVING_WORKLOAD = ("Poisson arrivals 200 jobs/s; N ~ U{10..300}, n_traj ~ U{1..256}, n_steps log-uniform "
                     "[1e3, 1e5], shear or uniaxial at U[0.1, 5], FENE b=100, h*=0.25 Chebyshev, write_every=100; "
                     "replayed in real time for the horizon; shortest-job-first admission under a 256-job queue "
@@ -240,7 +240,7 @@ def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
 
 
 def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed", queue_limit=256,
-                max_active=4096, drain=False, policy="sjf", slice_steps=100, slice_budget_s=1.0):
+                max_active=4096, drain=False, policy="sjf", slice_steps=100, slice_budget_s=1.0, drain_limit=None):
     """The serving workload: Poisson job arrivals replayed in real time
     against the continuous-batching server for `horizon` seconds. Jobs: N ~
     U{10..300}, n_traj ~ U{1..256}, n_steps log-uniform [1e3, 1e5] (times
@@ -259,7 +259,7 @@ def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed
                          hbm_budget_bytes=2 << 30, queue_limit=queue_limit, max_active_chains=max_active,
                          policy=policy, slice_steps=slice_steps, slice_budget_s=slice_budget_s)
     torch.cuda.synchronize()
-    st = srv.run_stream(jobs, np.asarray(arrivals), horizon=horizon, drain=drain)
+    st = srv.run_stream(jobs, np.asarray(arrivals), horizon=horizon, drain=drain, drain_limit=drain_limit)
     torch.cuda.synchronize()
     st.update({"jobs_offered": len(jobs), "horizon_s": horizon, "rate_jobs_per_s": rate,
                "n_steps_scale": scale_steps, "queue_limit": queue_limit, "max_active_chains": max_active,
@@ -485,7 +485,7 @@ def main():
         # of the same job mix that one GPU serves to completion
         serving = run_serving(torch, args.serving_seconds, seed=rank)
         light = run_serving(torch, LIGHT["horizon"], scale_steps=LIGHT["scale_steps"], rate=LIGHT["rate"],
-                            seed=rank + 1, drain=True)
+                            seed=rank + 1, drain=True, drain_limit=LIGHT["drain_limit"])
 
     if rank != 0:
         if dist is not None:
@@ -546,7 +546,8 @@ def main():
             print(json.dumps({"detail": name, **st}))
     print(json.dumps({"detail": "serving_workload", "overload": SERVING_WORKLOAD,
                       "light": f"the same job mix with n_steps x{LIGHT['scale_steps']} (min 100), "
-                               f"{LIGHT['rate']} jobs/s for {LIGHT['horizon']} s, drained"}))
+                               f"{LIGHT['rate']} jobs/s for {LIGHT['horizon']} s, drained for up to {LIGHT['drain_limit']} s "
+                               "(jobs still running then are censored samples)"}))
 
     def lat(st):
         if st is None:

@@ -5,6 +5,8 @@ oracle finishes in well under a second.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 from bdsim_b200 import initial
@@ -128,17 +130,84 @@ def build_case(name):
         R0 = initial.gaussian_chain(3, seed=14)
         sim = _sim(0.01, 15)
         seed = 14
+    elif name == "cheb_fallback_always":
+        # fd_err_max < 0: no Chebyshev series satisfies the fluctuation-
+        # dissipation check (its error is >= 0), so every step grows the
+        # series to MAXCHEB terms and falls back to the Cholesky factor
+        # (src/mobility.cpp:69-81). (With fd_err_max = 0 a series converged to
+        # machine precision can still pass, on an error of exactly 0.)
+        p.spring.type, p.spring.sqrtb = Spring.FENE, 50.0 ** 0.5
+        p.hstar, p.hi_method, p.fd_err_max = 0.25, DelSMethod.Chebyshev, -1.0
+        p.ev.type, p.ev.zstar, p.ev.dstar = EV.Gauss, 1.0, 0.5
+        p.flow = _shear(1.0)
+        R0 = initial.gaussian_chain(12, seed=21)
+        sim = _sim(1e-3, 8)
+        seed = 21
+    elif name == "corrector_cap_tol0":
+        # implicit_loop_tol = 0: the increment reaches exactly 0 at the fixed
+        # point, never below it, so every step runs the corrector to its
+        # 100N cap and is accepted as non-converged (src/integrator.cpp:140-163)
+        p.spring.type, p.spring.sqrtb = Spring.FENE, 5.0
+        p.hstar, p.hi_method = 0.2, DelSMethod.Cholesky
+        p.flow = _shear(2.0)
+        R0 = initial.gaussian_chain(8, bond_std=0.8, seed=22)
+        sim = _sim(1e-3, 5, tol=0.0)
+        seed = 22
+    elif name == "corrector_cap_stretched":
+        # the serving regime: FENE b=100 in uniaxial extension at rate 5 at
+        # full extension, where the reference's own corrector stops
+        # converging on most steps. R0 is the reference's state after 718
+        # steps from gaussian_chain(30, seed=31) with Rng(31) (prestates.npz).
+        stretched_physics(p)
+        R0 = prestate(name)
+        sim = _sim(1e-3, 12, t0=0.718)
+        seed = 42
+    elif name == "wlcbounded_sigma095":
+        # sigma = 0.95: the rtsafe bracket [2 sigma - 1, 1) of
+        # solve_wlc_bounded (src/spring.cpp:101-119) is 0.1 wide
+        p.spring.type, p.spring.sqrtb, p.spring.natural_length = Spring.WLCbounded, 6.0, 5.7
+        p.bend.type, p.bend.stiffness = Bending.OneMinusCosTheta, 1.0
+        R0 = initial.fene_fraenkel_chain(8, sigma=5.7, dQ=0.25, seed=24)
+        sim = _sim(0.01, 20)
+        seed = 24
     else:
         raise KeyError(name)
     p.number_of_beads = len(R0)
     return np.ascontiguousarray(R0, dtype=np.float64), p, sim, seed
 
 
+def stretched_physics(p):
+    """FENE b=100, h*=0.25 Chebyshev, uniaxial extension at rate 5."""
+    p.spring.type, p.spring.sqrtb = Spring.FENE, 10.0
+    p.hstar, p.hi_method = 0.25, DelSMethod.Chebyshev
+    p.flow = _uniaxial(5.0)
+
+
+PRESTATES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "prestates.npz")
+
+
+def prestate_spec(name):
+    """How the reference produced a family's starting state, with the
+    family's own physics: (beads, seed of gaussian_chain and of Rng, steps
+    from t = 0, dt)."""
+    return {"corrector_cap_stretched": (30, 31, 718, 1e-3)}[name]
+
+
+def prestate(name):
+    """A family's starting positions, made by the reference (see
+    prestate_spec) and stored in prestates.npz."""
+    with np.load(PRESTATES) as z:
+        return z[f"{name}/R0"].copy()
+
+
+# the families that take the reference's failure branches
+FAILURE_CASES = ["cheb_fallback_always", "corrector_cap_tol0", "corrector_cap_stretched", "wlcbounded_sigma095"]
+
 CASES = [
     "rouse_hook", "fene_free_shear_gauss", "cfg1_ff_cholesky", "cfg2_fene_cheb_gauss", "cfg3_wlc_lj_uniax",
     "cfg4_fene_b100_cheb", "cfg5_ff_bend_sdk_cheb", "cfg5_ff_bend_sdk_cholesky", "ilc_timeflow_external",
     "wlcbounded_free", "fraenkel_lj_equil_nocom", "n2_dumbbell_hi", "n3_bend_hi_chol",
-]
+] + FAILURE_CASES
 
 
 def build_large_case(name, N, n_steps=2, seed=0):

@@ -10,8 +10,10 @@
                       one multi-step call per case, and the same span taken
                       one step per call (per-step states, RNG states, times).
 
-Run here, where the reference sources exist:  python tests/golden/make_golden.py
-The GPU tests read only these files, never the reference tree.
+Run where the reference sources exist:
+    python tests/golden/make_golden.py [--ref REFERENCE_ROOT]
+(the root defaults to $BDSIM_REF, else /root/reference). The GPU tests read only
+these files, never the reference tree.
 """
 from __future__ import annotations
 
@@ -22,6 +24,14 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def reference_root() -> str:
+    """The bdsim checkout to read: --ref PATH, else $BDSIM_REF, else /root/reference."""
+    if "--ref" in sys.argv:
+        return sys.argv[sys.argv.index("--ref") + 1]
+    return os.environ.get("BDSIM_REF", "/root/reference")
+
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
@@ -176,7 +186,7 @@ def write_singular():
     """Extract R0_SINGULAR / SINGULAR_HSTAR from the reference's
     validation/compare_fortran_oracle.py into tests/golden/singular.py."""
     import re
-    src = open("/root/reference/validation/compare_fortran_oracle.py").read()
+    src = open(os.path.join(reference_root(), "validation", "compare_fortran_oracle.py")).read()
     m = re.search(r"R0_SINGULAR = np\.array\(\[(.*?)\]\)\s*\n\s*SINGULAR_HSTAR = ([0-9.eE+-]+)", src, re.S)
     rows = re.findall(r"\[([^\[\]]+)\]", m.group(1))
     arr = np.array([[float(v) for v in r.split(",")] for r in rows])
@@ -191,6 +201,46 @@ def write_singular():
         f.write("])\n\nSINGULAR_HSTAR = " + repr(float(m.group(2))) + "\n")
 
 
+COUNTERS = ["steps", "dx_products", "cheb_terms", "corrector_iters", "lanczos_cold", "lanczos_warm",
+            "cheb_fallbacks", "nonconverged"]
+
+
+def sensitivity(ref, R, phys, sim, rng, R_out):
+    """How far the reference's own result moves when one input coordinate
+    moves by one ulp: max over three coordinates of
+    max|R_out' - R_out| / max(1, max|R_out|). About 1e-18 where the step is
+    well conditioned; up to ~1e-8 where the corrector stops converging (its
+    iteration no longer contracts), which bounds what any other rounding of
+    the same step can reproduce."""
+    N = len(R)
+    worst = 0.0
+    for i, d in ((min(1, N - 1), 0), (N // 2, 1), (N - 1, 2)):
+        Rp = np.array(R, dtype=np.float64, copy=True)
+        Rp[i, d] = np.nextafter(Rp[i, d], np.inf)
+        Ro, _, _ = ref.integrate(Rp, phys, sim, rng)
+        worst = max(worst, float(np.max(np.abs(Ro - R_out)) / max(1.0, float(np.max(np.abs(R_out))))))
+    return worst
+
+
+def write_prestates(ref):
+    """Starting states of the families that begin mid-run, made by the
+    reference from a fresh chain (tests/golden/cases.py:prestate_spec)."""
+    from tests.golden.cases import PRESTATES, _sim, prestate_spec, stretched_physics
+    from bdsim_b200.params import PhysParams
+    from bdsim_b200 import initial
+    out = {}
+    for name in ("corrector_cap_stretched",):
+        N, seed, steps, dt = prestate_spec(name)
+        # the family's physics, from t = 0
+        p = PhysParams()
+        stretched_physics(p)
+        p.number_of_beads = N
+        R, _, status = ref.integrate(initial.gaussian_chain(N, seed=seed), p, _sim(dt, steps), (1, -1, seed))
+        assert status == 0
+        out[f"{name}/R0"] = R
+    np.savez_compressed(PRESTATES, **out)
+
+
 def main():
     write_singular()
     with open(os.path.join(HERE, "known_answers.json"), "w") as fh:
@@ -199,6 +249,8 @@ def main():
     if not O.ref_available():
         O.build()
     ref = O.ref()
+    port = O.port()
+    write_prestates(ref)
     arrays = {}
     for name in CASES:
         R0, phys, sim, seed = build_case(name)
@@ -207,31 +259,48 @@ def main():
         arrays[f"{name}/R1"] = R1
         arrays[f"{name}/rng"] = np.array(st1, dtype=np.int64)
         arrays[f"{name}/status"] = np.array(status)
+        # the non-fatal status bits and counters, which the reference only
+        # prints: from the C restatement, bitwise equal to the reference here
+        Rp, stp, sp, cp = port.integrate(R0, phys, sim, (1, -1, seed))
+        assert np.array_equal(Rp, R1) and stp == st1, name
+        arrays[f"{name}/port_status"] = np.array(sp)
+        arrays[f"{name}/port_counters"] = np.array([cp[k] for k in COUNTERS], dtype=np.int64)
+        arrays[f"{name}/sens"] = np.array(sensitivity(ref, R0, phys, sim, (1, -1, seed), R1))
         # the same span one reference step at a time: state k at time
         # t_k = t0 + k*dt -> state k+1 (each call a fresh model, cold cache)
         n = count_steps(sim)
         Rk, st = R0.copy(), (1, -1, seed)
         Rs, sts, ts = [Rk], [st], []
+        sstat, siters, ssens = [], [], []
         for k in range(n):
             one = SimParams()
             one.dt, one.implicit_loop_tol = sim.dt, sim.implicit_loop_tol
             one.update_center_of_mass = sim.update_center_of_mass
             one.time_start = one.time_end = sim.time_start + k * sim.dt
-            Rk, st, stt = ref.integrate(Rk, phys, one, st)
+            Rn, stn, stt = ref.integrate(Rk, phys, one, st)
             assert stt == 0
+            Rpn, stpn, spn, cpn = port.integrate(Rk, phys, one, st)
+            assert np.array_equal(Rpn, Rn) and stpn == stn, (name, k)
+            sstat.append(spn)
+            siters.append(cpn["corrector_iters"])
+            ssens.append(sensitivity(ref, Rk, phys, one, st, Rn))
+            Rk, st = Rn, stn
             Rs.append(Rk)
             sts.append(st)
             ts.append(one.time_start)
         arrays[f"{name}/steps/R"] = np.stack(Rs)
         arrays[f"{name}/steps/rng"] = np.array(sts, dtype=np.int64)
         arrays[f"{name}/steps/t"] = np.array(ts)
+        arrays[f"{name}/steps/status"] = np.array(sstat, dtype=np.int64)
+        arrays[f"{name}/steps/iters"] = np.array(siters, dtype=np.int64)
+        arrays[f"{name}/steps/sens"] = np.array(ssens)
     np.savez_compressed(os.path.join(HERE, "ref_steps.npz"), **arrays)
     print(f"wrote {len(CASES)} reference cases")
     # the reference's initial-configuration generators (python/bdsim/initial.py),
     # loaded by path: they need only numpy
     import importlib.util
     spec = importlib.util.spec_from_file_location("bdsim_ref_initial",
-                                                  "/root/reference/python/bdsim/initial.py")
+                                                  os.path.join(reference_root(), "python", "bdsim", "initial.py"))
     ri = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(ri)
     init = {}

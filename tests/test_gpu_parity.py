@@ -10,7 +10,17 @@ Tolerances, stated once:
                      changes by one ulp, and CUDA's libm differs from glibc's
                      by up to 2 ulp.
   MIXED_TOL = 1e-4   FP32-mixed form, per call of <= 40 steps, same norm
-RNG streams are compared bit for bit.
+  COND = 100         where a step (or call) is ill conditioned -- the
+                     corrector at its 100N cap, whose iteration no longer
+                     contracts -- the reference's own result moves by `sens`
+                     (up to ~1e-8, stored per step in the fixtures) when one
+                     input coordinate moves by one ulp; the bound there is
+                     max(PLAIN_TOL or CALL_TOL, COND * sens). A build of the
+                     C restatement with FMA contraction everywhere (every
+                     multiply-add rounded differently) stays within 4.2 x sens
+                     of the reference on every step of every family.
+RNG streams are compared bit for bit; per-step statuses and corrector
+iteration counts exactly.
 """
 import os
 
@@ -20,13 +30,14 @@ import pytest
 import bdsim_b200 as B
 from bdsim_b200 import _abi
 from bdsim_b200.params import DelSMethod, EV, PhysParams, Rng, SimParams, Spring
-from tests.golden.cases import CASES, build_case
+from tests.golden.cases import CASES, FAILURE_CASES, build_case
 
 pytestmark = pytest.mark.gpu
 
 PLAIN_TOL = 1e-12
 CALL_TOL = 1e-10
 MIXED_TOL = 1e-4
+COND = 100.0
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
@@ -67,13 +78,16 @@ def test_plain_every_step_matches_reference(fixtures):
     """Every step of every case, from the reference's own state, RNG state and
     time, as independent chains of one batch (cold spectral cache: each
     reference step is its own integrate call)."""
-    Rs, phys, sims, rngs, want, want_rng, tags = [], [], [], [], [], [], []
+    Rs, phys, sims, rngs, want, want_rng, tags, tols, stats, iters = [], [], [], [], [], [], [], [], [], []
     for name in CASES:
         _, p, s, _ = build_case(name)
         SR = fixtures[f"{name}/steps/R"]
         Srng = fixtures[f"{name}/steps/rng"]
         St = fixtures[f"{name}/steps/t"]
         for k in range(len(St)):
+            tols.append(max(PLAIN_TOL, COND * float(fixtures[f"{name}/steps/sens"][k])))
+            stats.append(int(fixtures[f"{name}/steps/status"][k]))
+            iters.append(int(fixtures[f"{name}/steps/iters"][k]))
             Rs.append(SR[k])
             phys.append(p)
             sims.append(_one_step_sim(s, float(St[k])))
@@ -83,15 +97,20 @@ def test_plain_every_step_matches_reference(fixtures):
             want.append(SR[k + 1])
             want_rng.append(tuple(int(v) for v in Srng[k + 1]))
             tags.append((name, k))
-    out, status, _ = B.integrate_many(Rs, phys, sims, rngs, form="plain")
-    worst = 0.0
+    out, status, cnt = B.integrate_many(Rs, phys, sims, rngs, form="plain")
+    worst, loose = 0.0, 0
     for i, tag in enumerate(tags):
-        assert status[i] == 0, tag
+        assert status[i] == stats[i], (tag, status[i], stats[i])
+        assert cnt[i]["corrector_iters"] == iters[i], (tag, cnt[i]["corrector_iters"], iters[i])
         assert rngs[i].state() == want_rng[i], tag
         e = rel(out[i], want[i])
-        worst = max(worst, e)
-        assert e <= PLAIN_TOL, (tag, e)
-    print(f"{len(tags)} reference steps, worst relative difference {worst:.2e}")
+        if tols[i] == PLAIN_TOL:
+            worst = max(worst, e)
+        else:
+            loose += 1
+        assert e <= tols[i], (tag, e, tols[i])
+    print(f"{len(tags)} reference steps, worst relative difference {worst:.2e} "
+          f"({loose} ill-conditioned capped steps at {COND:g} x the reference's 1-ulp sensitivity)")
 
 
 def test_plain_every_warm_step_matches_port(port):
@@ -139,9 +158,10 @@ def test_plain_call_matches_reference(name, fixtures):
     R0, p, s, seed = build_case(name)
     g = Rng(seed)
     out, status, _ = B.integrate_many([R0], p, s, [g], form="plain")
-    assert int(status[0]) == int(fixtures[f"{name}/status"])
+    assert int(status[0]) & _abi.ST_FATAL_MASK == int(fixtures[f"{name}/status"])
+    assert int(status[0]) == int(fixtures[f"{name}/port_status"])
     assert g.state() == tuple(int(v) for v in fixtures[f"{name}/rng"])
-    assert rel(out[0], fixtures[f"{name}/R1"]) <= CALL_TOL
+    assert rel(out[0], fixtures[f"{name}/R1"]) <= max(CALL_TOL, COND * float(fixtures[f"{name}/sens"]))
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -150,20 +170,61 @@ def test_plain_matches_port_with_counters(name, port):
     g = Rng(seed)
     out, status, cnt = B.integrate_many([R0], p, s, [g], form="plain")
     Rp, st, pst, pcnt = port.integrate(R0, p, s, (1, -1, seed))
-    assert rel(out[0], Rp) <= CALL_TOL
+    fx = np.load(os.path.join(GOLD, "ref_steps.npz"))
+    assert rel(out[0], Rp) <= max(CALL_TOL, COND * float(fx[f"{name}/sens"]))
     assert g.state() == st
-    for k in ("steps", "corrector_iters", "lanczos_cold", "lanczos_warm", "cheb_fallbacks"):
+    assert int(status[0]) == pst
+    for k in ("steps", "corrector_iters", "lanczos_cold", "lanczos_warm", "cheb_fallbacks", "nonconverged"):
         assert cnt[0][k] == pcnt[k], k
 
 
-@pytest.mark.parametrize("name", [c for c in CASES if "cholesky" not in c])
+@pytest.mark.parametrize("name", [c for c in CASES if "cholesky" not in c and c != "corrector_cap_stretched"])
 def test_mixed_close_to_reference(name, fixtures):
     R0, p, s, seed = build_case(name)
     g = Rng(seed)
     out, status, _ = B.integrate_many([R0], p, s, [g], form="mixed")
-    assert not (status[0] & _abi.ST_FATAL_MASK)
+    assert int(status[0]) == int(fixtures[f"{name}/port_status"])
     assert g.state() == tuple(int(v) for v in fixtures[f"{name}/rng"])  # same noise stream
     assert rel(out[0], fixtures[f"{name}/R1"]) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("name", FAILURE_CASES)
+def test_failure_branches_match_the_reference_in_both_forms(name, fixtures):
+    """Chebyshev -> Cholesky fallbacks and capped corrector steps: the same
+    statuses and the same counts as the reference (the C restatement, bitwise
+    equal to it on these families), in the plain and the FP32-mixed form,
+    from the reference's state at every step. In the stretched-chain regime
+    the capped corrector's result is ill conditioned (the reference moves by
+    up to ~1e-8 for a one-ulp input change), which no FP32 computation can
+    follow: the mixed form is held to the statuses and iteration counts
+    there, and to MIXED_TOL where the steps are well conditioned."""
+    _, p, s, _ = build_case(name)
+    SR, Srng, St = fixtures[f"{name}/steps/R"], fixtures[f"{name}/steps/rng"], fixtures[f"{name}/steps/t"]
+    want_st, want_it = fixtures[f"{name}/steps/status"], fixtures[f"{name}/steps/iters"]
+    sens = fixtures[f"{name}/steps/sens"]
+    n = len(St)
+    for form in ("plain", "mixed"):
+        rngs = []
+        for k in range(n):
+            g = Rng(0)
+            g.set_state(tuple(int(v) for v in Srng[k]))
+            rngs.append(g)
+        out, status, cnt = B.integrate_many([SR[k] for k in range(n)], p,
+                                            [_one_step_sim(s, float(St[k])) for k in range(n)], rngs, form=form)
+        for k in range(n):
+            assert int(status[k]) == int(want_st[k]), (form, k, status[k], want_st[k])
+            assert rngs[k].state() == tuple(int(v) for v in Srng[k + 1]), (form, k)
+            for c in ("cheb_fallbacks", "nonconverged"):
+                assert cnt[k][c] == (1 if c == "cheb_fallbacks" and want_st[k] & _abi.ST_CHEB_FALLBACK else
+                                     1 if c == "nonconverged" and want_st[k] & _abi.ST_NONCONVERGED else 0)
+            e = rel(out[k], SR[k + 1])
+            if form == "plain":
+                assert cnt[k]["corrector_iters"] == int(want_it[k]), (k, cnt[k]["corrector_iters"])
+                assert e <= max(PLAIN_TOL, COND * float(sens[k])), (k, e)
+            elif sens[k] < 1e-12:
+                assert e <= MIXED_TOL, (form, k, e)
+        if name != "wlcbounded_sigma095":
+            assert sum(c["cheb_fallbacks"] + c["nonconverged"] for c in cnt) > 0
 
 
 def test_forces_match_port(port):

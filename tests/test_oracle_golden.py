@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from bdsim_b200.params import Bending, DelSMethod, EV, PhysParams, Spring
-from tests.golden.cases import CASES, build_case
+from bdsim_b200 import _abi
+from tests.golden.cases import CASES, FAILURE_CASES, build_case
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 KNOWN = json.load(open(os.path.join(GOLD, "known_answers.json")))
@@ -112,10 +113,14 @@ def test_port_matches_reference_fixtures_bitwise(port, name):
     fx = np.load(os.path.join(GOLD, "ref_steps.npz"))
     R0, p, s, seed = build_case(name)
     assert np.array_equal(R0, fx[f"{name}/R0"])
-    R1, st, status, _ = port.integrate(R0, p, s, (1, -1, seed))
-    assert int(fx[f"{name}/status"]) == status
+    R1, st, status, cnt = port.integrate(R0, p, s, (1, -1, seed))
+    # the reference reports only the fatal bits (as exceptions); the port
+    # adds the non-fatal ones (non-converged steps, Chebyshev fallbacks)
+    assert int(fx[f"{name}/status"]) == status & _abi.ST_FATAL_MASK
+    assert int(fx[f"{name}/port_status"]) == status
     assert np.array_equal(R1, fx[f"{name}/R1"]), np.max(np.abs(R1 - fx[f"{name}/R1"]))
     assert tuple(int(v) for v in fx[f"{name}/rng"]) == st
+    assert [cnt[k] for k in _abi.COUNTER_FIELDS] == [int(v) for v in fx[f"{name}/port_counters"]]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -129,8 +134,39 @@ def test_port_matches_reference_step_by_step_bitwise(port, name):
         one.dt, one.implicit_loop_tol = s.dt, s.implicit_loop_tol
         one.update_center_of_mass = s.update_center_of_mass
         one.time_start = one.time_end = float(St[k])
-        R1, st, status, _ = port.integrate(SR[k], p, one, tuple(int(v) for v in Srng[k]))
-        assert status == 0 and np.array_equal(R1, SR[k + 1]) and st == tuple(int(v) for v in Srng[k + 1])
+        R1, st, status, cnt = port.integrate(SR[k], p, one, tuple(int(v) for v in Srng[k]))
+        assert status == int(fx[f"{name}/steps/status"][k]), (k, status)
+        assert cnt["corrector_iters"] == int(fx[f"{name}/steps/iters"][k]), k
+        assert np.array_equal(R1, SR[k + 1]) and st == tuple(int(v) for v in Srng[k + 1]), k
+
+
+@pytest.mark.parametrize("name", FAILURE_CASES)
+def test_failure_families_take_the_failure_branches(name):
+    """The fixtures of these families show the branches they exist for: the
+    Chebyshev -> Cholesky fallback, the corrector's 100N cap (in the
+    deterministic tol = 0 form and in the stretched-chain regime where the
+    reference's own iteration stops contracting), and rtsafe on a narrow
+    WLC-bounded bracket."""
+    fx = np.load(os.path.join(GOLD, "ref_steps.npz"))
+    cnt = dict(zip(_abi.COUNTER_FIELDS, (int(v) for v in fx[f"{name}/port_counters"])))
+    steps = fx[f"{name}/steps/status"]
+    if name == "cheb_fallback_always":
+        assert cnt["cheb_fallbacks"] == cnt["steps"] > 0 and all(s & _abi.ST_CHEB_FALLBACK for s in steps)
+    elif name == "corrector_cap_tol0":
+        _, p, _, _ = build_case(name)
+        assert cnt["nonconverged"] == cnt["steps"] > 0
+        assert all(int(i) == 100 * p.number_of_beads + 1 for i in fx[f"{name}/steps/iters"])
+    elif name == "corrector_cap_stretched":
+        capped = [(int(s) & _abi.ST_NONCONVERGED) != 0 for s in steps]
+        assert 0 < sum(capped) < len(capped)  # both branches
+        # where the corrector is capped the reference's own result moves by
+        # far more than an ulp when its input moves by one ulp
+        sens = fx[f"{name}/steps/sens"]
+        assert max(sens[capped]) > 1e-12 > max(sens[[not c for c in capped]])
+    else:
+        _, p, _, _ = build_case(name)
+        assert p.spring.natural_length / p.spring.sqrtb == pytest.approx(0.95)
+        assert cnt["corrector_iters"] > cnt["steps"]
 
 
 def test_port_matches_live_reference_components(port, ref):
