@@ -93,7 +93,7 @@ class BdcuBucketInfo(ctypes.Structure):
     """One bucket of a launch plan (bdcu_bucket_info)."""
     _fields_ = [(k, ctypes.c_int32) for k in (
         "bucket", "kernel", "team_warps", "n_chains", "min_beads", "max_beads", "block", "grid", "v_cap",
-        "d_in_smem", "tuned", "reserved")] + [("smem_bytes", ctypes.c_int64)]
+        "d_in_smem", "tuned", "team_beads_per_thread")] + [("smem_bytes", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -283,9 +283,10 @@ def load_library():
                                        ctypes.POINTER(BdcuSim), c_int64_p]
     lib.bdcu_write_arena.argtypes = [vp, ctypes.c_int64, c_double_p, ctypes.c_int64]
     lib.bdcu_select.argtypes = [vp, ctypes.c_int, c_int32_p]
+    lib.bdcu_set_team_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.bdcu_check_chains.argtypes = [ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim), c_double_p,
                                       ctypes.c_int64, ctypes.c_char_p, ctypes.c_int]
-    for name in ("bdcu_check_chains", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
+    for name in ("bdcu_set_team_shape", "bdcu_check_chains", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
                  "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
                  "bdcu_forces", "bdcu_ran1", "bdcu_run_static", "bdcu_describe_plan", "bdcu_autotune",
                  "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select"):
@@ -300,7 +301,7 @@ EXPORTED_SYMBOLS = [
     "bdcu_set_chains", "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host",
     "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_describe_plan", "bdcu_autotune",
     "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select", "bdcu_run_static",
-    "bdcu_check_chains",
+    "bdcu_check_chains", "bdcu_set_team_shape",
 ]
 
 

@@ -21,8 +21,8 @@ cudaError_t launch_plain(const RunArgs& a, int grid, int block, size_t smem, cud
 cudaError_t launch_mixed(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t occupancy_plain(int block, size_t smem, int* per_sm);
 cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm);
-cudaError_t launch_mixed_team(int team_warps, const RunArgs& a, int grid, size_t smem, cudaStream_t s);
-cudaError_t occupancy_mixed_team(int team_warps, size_t smem, int* per_sm);
+cudaError_t launch_mixed_team(int team_warps, int team_q, const RunArgs& a, int grid, size_t smem, cudaStream_t s);
+cudaError_t occupancy_mixed_team(int team_warps, int team_q, size_t smem, int* per_sm);
 cudaError_t launch_forces(const DevChain* chains, int n_chains, int n_max, const double* arena, const double* R,
                           double t, int which, double* F, cudaStream_t s);
 cudaError_t launch_ran1(int n_chains, int32_t* rng, int n_per, double* out, cudaStream_t s);
@@ -325,13 +325,18 @@ int fill_launch(bdcu_ctx* ctx, int form, Bucket& b, const Shape* s) {
     int per_sm = 0;
     cudaError_t e;
     if (b.kernel == BDCU_KERNEL_TEAM) {
-        const int T = b.team_warps;
-        b.smem = (size_t)team_smem(T, b.n_max);
+        if (s && s->team_warps > 0) {
+            b.team_warps = s->team_warps;
+            b.team_q = s->team_q;
+        }
+        const int T = b.team_warps, Q = b.team_q;
+        if (!team_shape_fits(T, Q, b.max_beads)) return fail(ctx, BDCU_E_ARG, "team shape does not hold the bucket");
+        b.smem = (size_t)team_smem(T, Q, b.n_max);
         if (b.smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "team kernel shared memory exceeds the device limit");
-        e = occupancy_mixed_team(T, b.smem, &per_sm);
+        e = occupancy_mixed_team(T, Q, b.smem, &per_sm);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "occupancy_mixed_team");
         if (per_sm < 1) return fail(ctx, BDCU_E_LIMIT, "team kernel cannot be resident");
-        const int tpc = teams_per_cta(T);
+        const int tpc = teams_per_cta(T, Q);
         b.block = 32 * T * tpc;
         b.grid = std::max(1, std::min((b.count + tpc - 1) / tpc, per_sm * ctx->sm_count));
         b.v_cap = 0;
@@ -370,7 +375,7 @@ int ensure_async(bdcu_ctx* ctx, T** p, size_t count, size_t* cap_bytes) {
 }
 
 int ensure_bucket_scratch(bdcu_ctx* ctx, const Bucket& b) {
-    const int per = b.kernel == BDCU_KERNEL_TEAM ? teams_per_cta(b.team_warps) : 1;
+    const int per = b.kernel == BDCU_KERNEL_TEAM ? teams_per_cta(b.team_warps, b.team_q) : 1;
     const size_t doubles = (size_t)b.scratch_stride * b.grid * per;
     return ensure_async(ctx, &ctx->bscratch[b.id], doubles, &ctx->bscratch_bytes[b.id]);
 }
@@ -401,6 +406,7 @@ int build_plan(bdcu_ctx* ctx, int form) {
         b.id = id;
         b.kernel = id < kFirstBlockBucket ? BDCU_KERNEL_TEAM : BDCU_KERNEL_BLOCK;
         b.team_warps = id < kFirstBlockBucket ? (1 << id) : 0;
+        b.team_q = id < kFirstBlockBucket ? 2 : 0;
         b.count = (int)L.size();
         b.max_beads = ctx->chains_h[L.front()].N;
         b.min_beads = ctx->chains_h[L.back()].N;
@@ -416,7 +422,10 @@ int build_plan(bdcu_ctx* ctx, int form) {
         b.order_off = (int64_t)ctx->order_h.size();
         ctx->order_h.insert(ctx->order_h.end(), L.begin(), L.end());
         if (b.kernel == BDCU_KERNEL_TEAM) {
-            if ((rc = fill_launch(ctx, form, b, nullptr))) return rc;
+            const Shape& t = ctx->tuned[mixed][id];
+            const bool use = t.team_warps > 0 && team_shape_fits(t.team_warps, t.team_q, b.max_beads);
+            if ((rc = fill_launch(ctx, form, b, use ? &t : nullptr))) return rc;
+            b.tuned = use ? 1 : 0;
         } else {
             const std::vector<Shape> shapes = block_shapes(ctx, b, form);
             if (shapes.empty()) return fail(ctx, BDCU_E_LIMIT, "chain too large for the shared-memory layout");
@@ -509,7 +518,7 @@ int launch_bucket(bdcu_ctx* ctx, int form, const Bucket& b, const State& st, int
     a.bounds_every = form == BDCU_FORM_MIXED_FP32 ? ctx->bounds_every : 1;
     cudaError_t e;
     if (b.kernel == BDCU_KERNEL_TEAM)
-        e = launch_mixed_team(b.team_warps, a, b.grid, b.smem, s);
+        e = launch_mixed_team(b.team_warps, b.team_q, a, b.grid, b.smem, s);
     else
         e = (form == BDCU_FORM_MIXED_FP32) ? launch_mixed(a, b.grid, b.block, b.smem, s)
                                            : launch_plain(a, b.grid, b.block, b.smem, s);
@@ -732,7 +741,7 @@ int bdcu_describe_plan(bdcu_ctx* ctx, int form, bdcu_bucket_info* out, int cap, 
         o.bucket = b.id;
         o.kernel = b.kernel;
         o.team_warps = b.team_warps;
-        o.reserved = 0;
+        o.team_beads_per_thread = b.team_q;
         o.n_chains = b.count;
         o.min_beads = b.min_beads;
         o.max_beads = b.max_beads;
@@ -759,9 +768,6 @@ int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, 
     ctx->plan_dirty = 1;
     int rc = build_plan(ctx, form);
     if (rc) return rc;
-    bool any_block = false;
-    for (const Bucket& b : ctx->plan) any_block = any_block || b.kernel == BDCU_KERNEL_BLOCK;
-    if (!any_block) return BDCU_OK;
 
     const int64_t nb = std::max<int64_t>(ctx->bead_capacity, 1), nc = ctx->n_chains;
     double *tR = nullptr, *tcache = nullptr, *tt0 = nullptr;
@@ -803,10 +809,24 @@ int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, 
     cudaStream_t s = ctx->stream;
     const std::vector<Bucket> plan = ctx->plan;
     for (const Bucket& base : plan) {
-        if (base.kernel != BDCU_KERNEL_BLOCK) continue;
         float best_ms = 1e30f;
         Shape best;
-        for (const Shape& shape : block_shapes(ctx, base, form)) {
+        std::vector<Shape> shapes;
+        if (base.kernel == BDCU_KERNEL_BLOCK) {
+            shapes = block_shapes(ctx, base, form);
+        } else {
+            // team shapes that hold any chain of the bucket, up to twice its width
+            for (int i = 0; i < kNumTeamShapes; ++i) {
+                const int T = kTeamShapes[i][0], Q = kTeamShapes[i][1];
+                if (team_shape_fits(T, Q, kBucketBeads[base.id]) && 32 * T * Q <= 2 * kBucketBeads[base.id]) {
+                    Shape sh;
+                    sh.team_warps = T;
+                    sh.team_q = Q;
+                    shapes.push_back(sh);
+                }
+            }
+        }
+        for (const Shape& shape : shapes) {
             Bucket b = base;
             if (fill_launch(ctx, form, b, &shape) != BDCU_OK) continue;  // not resident: skip the shape
             if ((rc = ensure_bucket_scratch(ctx, b))) {
@@ -838,10 +858,25 @@ int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, 
                 best = shape;
             }
         }
-        if (best.block > 0) ctx->tuned[mixed][base.id] = best;
+        if (best.block > 0 || best.team_warps > 0) ctx->tuned[mixed][base.id] = best;
     }
 #undef TK
     cleanup();
+    ctx->plan_dirty = 1;
+    return BDCU_OK;
+}
+
+int bdcu_set_team_shape(bdcu_ctx* ctx, int bucket, int team_warps, int beads_per_thread) {
+    if (!ctx) return BDCU_E_ARG;
+    if (bucket < 0 || bucket >= kFirstBlockBucket) return fail(ctx, BDCU_E_ARG, "team buckets are 0..3");
+    Shape sh;
+    if (team_warps != 0) {
+        if (!team_shape_fits(team_warps, beads_per_thread, kBucketBeads[bucket]))
+            return fail(ctx, BDCU_E_ARG, "not a compiled team shape that holds every chain of the bucket");
+        sh.team_warps = team_warps;
+        sh.team_q = beads_per_thread;
+    }
+    ctx->tuned[1][bucket] = sh;
     ctx->plan_dirty = 1;
     return BDCU_OK;
 }

@@ -23,18 +23,22 @@ constexpr int kMaxBuckets = 8;
 constexpr int kFirstBlockBucket = 4;
 constexpr int kBucketBeads[kMaxBuckets] = {64, 128, 256, 512, 64, 128, 256, kMaxBeads};
 
-// A launch shape chosen by bdcu_autotune (block kernel): threads per block,
-// Lanczos vectors in shared memory, dense D in shared memory.
+// A launch shape chosen by bdcu_autotune. Block kernel: threads per block,
+// Lanczos vectors in shared memory, dense D in shared memory. Team kernel:
+// warps per team and beads per thread.
 struct Shape {
     int block = 0;  // 0: not tuned
     int v_cap = -1;
     int d_in_smem = -1;
+    int team_warps = 0;
+    int team_q = 0;
 };
 
 struct Bucket {
     int id = 0;
     int kernel = BDCU_KERNEL_BLOCK;
     int team_warps = 0;  // team kernel: warps per chain
+    int team_q = 0;      // team kernel: beads per thread
     int count = 0, min_beads = 0, max_beads = 0;
     int n_max = 0;  // 3 * max_beads
     int need_chol = 0, need_d = 0, need_lz = 0;

@@ -1,6 +1,7 @@
 // integrator_mixed.cu -- the FP32-mixed form (FMA contraction on).
 #include "integrator.cuh"
 #include "integrator_team.cuh"
+#include "plan.h"
 
 namespace bdcu {
 
@@ -27,38 +28,30 @@ cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, block, smem);
 }
 
-template <int T>
+template <int T, int Q>
 static cudaError_t launch_team_t(const RunArgs& a, int grid, size_t smem, cudaStream_t s) {
-    integrate_team_kernel<T><<<grid, TeamCfg<T>::kCtaThreads, smem, s>>>(a);
+    integrate_team_kernel<T, Q><<<grid, TeamCfg<T, Q>::kCtaThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <int T>
+template <int T, int Q>
 static cudaError_t occupancy_team_t(size_t smem, int* per_sm) {
-    cudaError_t e = allow_max_smem(reinterpret_cast<const void*>(integrate_team_kernel<T>));
+    cudaError_t e = allow_max_smem(reinterpret_cast<const void*>(integrate_team_kernel<T, Q>));
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, integrate_team_kernel<T>, TeamCfg<T>::kCtaThreads,
-                                                         smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, integrate_team_kernel<T, Q>,
+                                                         TeamCfg<T, Q>::kCtaThreads, smem);
 }
 
-cudaError_t launch_mixed_team(int team_warps, const RunArgs& a, int grid, size_t smem, cudaStream_t s) {
-    switch (team_warps) {
-        case 1: return launch_team_t<1>(a, grid, smem, s);
-        case 2: return launch_team_t<2>(a, grid, smem, s);
-        case 4: return launch_team_t<4>(a, grid, smem, s);
-        case 8: return launch_team_t<8>(a, grid, smem, s);
-        default: return cudaErrorInvalidValue;
-    }
+cudaError_t launch_mixed_team(int team_warps, int team_q, const RunArgs& a, int grid, size_t smem, cudaStream_t s) {
+#define BDCU_LAUNCH(t, q) launch_team_t<t, q>(a, grid, smem, s)
+    return BDCU_TEAM_SHAPE_SWITCH(team_warps, team_q, BDCU_LAUNCH, cudaErrorInvalidValue);
+#undef BDCU_LAUNCH
 }
 
-cudaError_t occupancy_mixed_team(int team_warps, size_t smem, int* per_sm) {
-    switch (team_warps) {
-        case 1: return occupancy_team_t<1>(smem, per_sm);
-        case 2: return occupancy_team_t<2>(smem, per_sm);
-        case 4: return occupancy_team_t<4>(smem, per_sm);
-        case 8: return occupancy_team_t<8>(smem, per_sm);
-        default: return cudaErrorInvalidValue;
-    }
+cudaError_t occupancy_mixed_team(int team_warps, int team_q, size_t smem, int* per_sm) {
+#define BDCU_OCC(t, q) occupancy_team_t<t, q>(smem, per_sm)
+    return BDCU_TEAM_SHAPE_SWITCH(team_warps, team_q, BDCU_OCC, cudaErrorInvalidValue);
+#undef BDCU_OCC
 }
 
 }  // namespace bdcu

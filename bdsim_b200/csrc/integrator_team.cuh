@@ -242,11 +242,11 @@ static __device__ void wk_tridiag_vec(const double* a, const double* b, int m, d
 }
 
 
-template <int T>
+template <int T, int Q>
 struct TeamChain {
     static constexpr int TT = 32 * T;  // threads of the team
     const RunArgs& a;
-    TeamShared<T>& S;
+    TeamShared<T, Q>& S;
     const DevChain& ch;
     double* V;      // warm Lanczos basis in shared memory (kLanczosWarm x nv)
     float* sqx;     // Chebyshev node values, aliasing V (dead after the bounds)
@@ -266,7 +266,7 @@ struct TeamChain {
     // rho = h*/r alone.
     float scale, iscale, K1, K2, K3, C3, C7;
 
-    __device__ TeamChain(const RunArgs& a_, TeamShared<T>& S_, const DevChain& ch_) : a(a_), S(S_), ch(ch_) {}
+    __device__ TeamChain(const RunArgs& a_, TeamShared<T, Q>& S_, const DevChain& ch_) : a(a_), S(S_), ch(ch_) {}
 
     __device__ __forceinline__ bool valid(int q) const { return tid + TT * q < N; }
     __device__ __forceinline__ int bead(int q) const { return tid + TT * q; }
@@ -358,22 +358,23 @@ struct TeamChain {
     // Inputs are staged in S.xs and, for K > 1, in S.s1 / S.s2 viewed as
     // float4 (free while the mobility products run).
     template <int K>
-    __device__ void applyK(const float (&x)[K][2][3], float (&acc)[K][2][3]) {
+    __device__ void applyK(const float (&x)[K][Q][3], float (&acc)[K][Q][3]) {
         static_assert(K >= 1 && K <= 3, "applyK stages at most three inputs");
-        static_assert(offsetof(TeamShared<T>, s1) % 16 == 0 && offsetof(TeamShared<T>, s2) % 16 == 0 &&
-                          sizeof(TeamShared<T>::s1) >= sizeof(float4) * 64 * T,
+        using Shared = TeamShared<T, Q>;
+        static_assert(offsetof(Shared, s1) % 16 == 0 && offsetof(Shared, s2) % 16 == 0 &&
+                          sizeof(Shared::s1) >= sizeof(float4) * 32 * T * Q,
                       "s1 / s2 must hold a 16-byte aligned float4 per bead");
         cnt[C_DX] += K;
         float4* stage[3] = {S.xs, reinterpret_cast<float4*>(S.s1), reinterpret_cast<float4*>(S.s2)};
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
             if (valid(q))
 #pragma unroll
                 for (int r = 0; r < K; ++r) stage[r][bead(q)] = make_float4(x[r][q][0], x[r][q][1], x[r][q][2], 0.f);
         sync();
-        float4 pb[2];
+        float4 pb[Q];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < Q; ++q) {
             pb[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
             for (int r = 0; r < K; ++r)
@@ -387,8 +388,8 @@ struct TeamChain {
         // to 1e-24) takes the near branch with om1 = 1 exactly in FP32 and
         // om2 d = 0: it contributes the identity block.
         bool one_slot = false;
-        if constexpr (T > 1) one_slot = __all_sync(kFull, !valid(1));
-        const int nq = one_slot ? 1 : 2;
+        if constexpr (T > 1 && Q == 2) one_slot = __all_sync(kFull, !valid(1));
+        const int nq = one_slot ? 1 : Q;
         // not unrolled: this loop is inlined at every product's call site, and
         // the smaller code measured 6% faster on the 4096 x N=50 workload
         // (fewer instruction-fetch stalls) despite a few more register spills
@@ -399,7 +400,7 @@ struct TeamChain {
 #pragma unroll
             for (int r = 0; r < K; ++r) xj[r] = stage[r][j];
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 if (q < nq) {
                     const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
                     const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
@@ -420,7 +421,7 @@ struct TeamChain {
         }
         sync();
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
             if (!valid(q))
 #pragma unroll
                 for (int r = 0; r < K; ++r)
@@ -428,35 +429,35 @@ struct TeamChain {
                     for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
     }
 
-    __device__ void apply32(const float (&x)[2][3], float (&acc)[2][3]) {
-        applyK<1>(reinterpret_cast<const float(&)[1][2][3]>(x), reinterpret_cast<float(&)[1][2][3]>(acc));
+    __device__ void apply32(const float (&x)[Q][3], float (&acc)[Q][3]) {
+        applyK<1>(reinterpret_cast<const float(&)[1][Q][3]>(x), reinterpret_cast<float(&)[1][Q][3]>(acc));
     }
 
-    __device__ void apply(const double (&x)[2][3], double (&y)[2][3]) {
+    __device__ void apply(const double (&x)[Q][3], double (&y)[Q][3]) {
         if (!hi) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) y[q][d] = x[q][d];
             return;
         }
-        float xf[2][3], yf[2][3];
+        float xf[Q][3], yf[Q][3];
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) xf[q][d] = (float)x[q][d];
         apply32(xf, yf);
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) y[q][d] = (double)yf[q][d];
     }
 
     // D.x on FP32 thread vectors (identity without HI).
-    __device__ void applyF(const float (&x)[2][3], float (&y)[2][3]) {
+    __device__ void applyF(const float (&x)[Q][3], float (&y)[Q][3]) {
         if (!hi) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) y[q][d] = x[q][d];
             return;
@@ -464,37 +465,37 @@ struct TeamChain {
         apply32(x, y);
     }
 
-    __device__ double dotf(const float (&x)[2][3], const float (&y)[2][3]) const {
+    __device__ double dotf(const float (&x)[Q][3], const float (&y)[Q][3]) const {
         double s = 0.0;
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) s += (double)x[q][d] * (double)y[q][d];
         return tsum(s);
     }
 
-    __device__ double dot(const double (&x)[2][3], const double (&y)[2][3]) const {
+    __device__ double dot(const double (&x)[Q][3], const double (&y)[Q][3]) const {
         double s = 0.0;
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) s += x[q][d] * y[q][d];
         return tsum(s);
     }
 
-    __device__ void stage_pos(const double (&R)[2][3]) {
+    __device__ void stage_pos(const double (&R)[Q][3]) {
         sync();
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
             if (valid(q))
                 S.pos[bead(q)] = make_float4((float)(R[q][0] * iscale), (float)(R[q][1] * iscale),
                                              (float)(R[q][2] * iscale), 0.f);
         sync();
     }
 
-    __device__ void to_smem(double* buf, const double (&x)[2][3]) const {
+    __device__ void to_smem(double* buf, const double (&x)[Q][3]) const {
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
             if (valid(q))
 #pragma unroll
                 for (int d = 0; d < 3; ++d) buf[3 * bead(q) + d] = x[q][d];
@@ -503,14 +504,14 @@ struct TeamChain {
     // ---- forces at R (FP64 springs/bending/external, FP32 EV) ------------
     // Fs: spring bead forces (src/spring.cpp:195-207). Fe: (EV + bending) +
     // external(t) (src/model.hpp:56-64). Positions must be staged (S.pos).
-    __device__ void forces(const double (&R)[2][3], double t, float (&Fs)[2][3], float (&Fe)[2][3], bool spring) {
+    __device__ void forces(const double (&R)[Q][3], double t, float (&Fs)[Q][3], float (&Fe)[Q][3], bool spring) {
         const bool bend = ch.bend_type != BDCU_BEND_NONE && N > 2;
         const bool bonds = spring || bend;  // bond forces, unit bonds, lengths: springs and bending only
         if (bonds) to_smem(S.s0, R);
         sync();
         // bonds b = bead(0), bead(1) (b < N-1): Fc -> s1, unit bonds -> s2, lengths -> s3
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < Q; ++q) {
             const int b = bead(q);
             if (bonds && b < N - 1) {
                 const double b0 = S.s0[3 * b + 3] - S.s0[3 * b], b1 = S.s0[3 * b + 4] - S.s0[3 * b + 1],
@@ -530,7 +531,7 @@ struct TeamChain {
         sync();
         if (bend) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 const int b = bead(q);
                 if (b < N - 2)
                     S.s4[b] = S.s2[3 * (b + 1)] * S.s2[3 * b] + S.s2[3 * (b + 1) + 1] * S.s2[3 * b + 1] +
@@ -543,17 +544,17 @@ struct TeamChain {
         const double* phi = (ch.ev_type == BDCU_EV_SDK && ch.phi_off >= 0) ? a.arena + ch.phi_off : nullptr;
         // excluded volume, FP32 pair sums over both bead slots at once: the
         // force on m from j is -fac(r) (R_j - R_m), |j - m| >= contour distance
-        float fev[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float fev[Q][3] = {};
         if (ch.ev_type == BDCU_EV_GAUSS) {
-            float4 pm[2];
+            float4 pm[Q];
 #pragma unroll
-            for (int q = 0; q < 2; ++q) pm[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int q = 0; q < Q; ++q) pm[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
             const int cd = ch.cd;
 #pragma unroll 2
             for (int j = 0; j < N; ++j) {
                 const float4 pj = S.pos[j];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
+                for (int q = 0; q < Q; ++q) {
                     const int m = bead(q);
                     const float dx = pj.x - pm[q].x, dy = pj.y - pm[q].y, dz = pj.z - pm[q].z;
                     const float sq = dx * dx + dy * dy + dz * dz;
@@ -566,7 +567,7 @@ struct TeamChain {
             }
         } else if (ch.ev_type != BDCU_EV_NONE) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 const int m = bead(q);
                 if (!valid(q)) continue;
                 const float4 pm = S.pos[m];
@@ -586,7 +587,7 @@ struct TeamChain {
             }
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < Q; ++q) {
             const int m = bead(q);
             if (!valid(q)) {
                 for (int d = 0; d < 3; ++d) Fs[q][d] = Fe[q][d] = 0.f;
@@ -615,7 +616,7 @@ struct TeamChain {
     // The team's threads draw contiguous blocks of the stream; thread u jumps
     // to draw u*c with the tabulated powers, so the uniforms equal ran_1's,
     // bit for bit.
-    __device__ void noise(uint32_t& ux0, int32_t& iy0, int32_t& seed, float (&X)[2][3]) {
+    __device__ void noise(uint32_t& ux0, int32_t& iy0, int32_t& seed, float (&X)[Q][3]) {
         if (seed <= 0 || iy0 < 0) {
             const int32_t s = seed < 0 ? -seed : seed;
             iy0 = (888889999 ^ s) | 1;
@@ -661,7 +662,7 @@ struct TeamChain {
             iy0 = S.bi;
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 double v = 0.0;
@@ -676,15 +677,15 @@ struct TeamChain {
 
     // ---- Lanczos extreme eigenvalues (src/hydrodynamics.cpp:146-264) ----
     __device__ double* basis(int j, int m) { return (m <= kLanczosWarm ? V : Vg) + (int64_t)j * nv; }
-    __device__ void load(const double* vec, double (&x)[2][3]) const {
+    __device__ void load(const double* vec, double (&x)[Q][3]) const {
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) x[q][d] = valid(q) ? vec[3 * bead(q) + d] : 0.0;
     }
-    __device__ void store(double* vec, const double (&x)[2][3]) const {
+    __device__ void store(double* vec, const double (&x)[Q][3]) const {
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
             if (valid(q))
 #pragma unroll
                 for (int d = 0; d < 3; ++d) vec[3 * bead(q) + d] = x[q][d];
@@ -693,7 +694,7 @@ struct TeamChain {
     // Lanczos start vector (src/hydrodynamics.cpp:152-155): the normalised
     // warm-start cache, or the normalised default seed when cold or when the
     // cache is zero.
-    __device__ void start_vector(bool warm, const double* cache, double (&v)[2][3]) const {
+    __device__ void start_vector(bool warm, const double* cache, double (&v)[Q][3]) const {
         double nv2 = 0.0;
         if (warm) {
             load(cache, v);
@@ -705,7 +706,7 @@ struct TeamChain {
         }
         const double inv = 1.0 / nv2;
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) v[q][d] *= inv;
     }
@@ -713,16 +714,16 @@ struct TeamChain {
     // Returns the number of Lanczos steps; sets rmin/rmax and the Ritz vectors.
     // v0: the start vector; if have_dv0, dv0 = D v0 (computed by the caller
     // together with the step's other independent products).
-    __device__ int lanczos(int m, bool warm, const double (&v0)[2][3], const double (&dv0)[2][3], bool have_dv0,
-                           double (&vmin)[2][3], double (&vmax)[2][3], double& rmin, double& rmax) {
+    __device__ int lanczos(int m, bool warm, const double (&v0)[Q][3], const double (&dv0)[Q][3], bool have_dv0,
+                           double (&vmin)[Q][3], double (&vmax)[Q][3], double& rmin, double& rmax) {
         if (n < m) m = n;
-        double v[2][3], w[2][3], vp[2][3];
+        double v[Q][3], w[Q][3], vp[Q][3];
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) v[q][d] = v0[q][d];
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) vp[q][d] = 0.0;
         int k = 0;
@@ -742,7 +743,7 @@ struct TeamChain {
                 store(basis(j, m), v);
                 if (j == 0 && have_dv0) {
 #pragma unroll
-                    for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < Q; ++q)
 #pragma unroll
                         for (int d = 0; d < 3; ++d) w[q][d] = dv0[q][d];
                 } else {
@@ -750,14 +751,14 @@ struct TeamChain {
                 }
                 if (j > 0)
 #pragma unroll
-                    for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < Q; ++q)
 #pragma unroll
                         for (int d = 0; d < 3; ++d) w[q][d] -= b * vp[q][d];
                 double c[kLanczosWarm];
 #pragma unroll
                 for (int u = 0; u < kLanczosWarm; ++u) c[u] = 0.0;
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         c[0] += v[q][d] * w[q][d];
@@ -766,7 +767,7 @@ struct TeamChain {
                 tsum8(c);
                 const double al = c[0];
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) w[q][d] -= al * v[q][d];
                 if (tid == 0) S.alpha[k] = al;
@@ -778,7 +779,7 @@ struct TeamChain {
                 if (b < 1.0e-10) break;
                 const double ib = 1.0 / b;
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         vp[q][d] = v[q][d];
@@ -792,7 +793,7 @@ struct TeamChain {
                 store(basis(j, m), v);
                 if (j == 0 && have_dv0) {
 #pragma unroll
-                    for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < Q; ++q)
 #pragma unroll
                         for (int d = 0; d < 3; ++d) w[q][d] = dv0[q][d];
                 } else {
@@ -802,16 +803,16 @@ struct TeamChain {
                 if (tid == 0) S.alpha[k] = al;
                 ++k;
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) w[q][d] -= al * v[q][d] + b * vp[q][d];
                 sync();
                 for (int u = 0; u <= j; ++u) {
-                    double uu[2][3];
+                    double uu[Q][3];
                     load(basis(u, m), uu);
                     const double dd = dot(w, uu);
 #pragma unroll
-                    for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < Q; ++q)
 #pragma unroll
                         for (int d = 0; d < 3; ++d) w[q][d] -= dd * uu[q][d];
                 }
@@ -819,7 +820,7 @@ struct TeamChain {
                 if (b < 1.0e-10) break;
                 const double ib = 1.0 / b;
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         vp[q][d] = v[q][d];
@@ -893,15 +894,15 @@ struct TeamChain {
         rmin = S.rr[0];
         rmax = S.rr[1];
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) vmin[q][d] = vmax[q][d] = 0.0;
         for (int j = 0; j < k; ++j) {
-            double vj[2][3];
+            double vj[Q][3];
             load(basis(j, m), vj);
             const double y1 = S.ymin[j], y2 = S.ymax[j];
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     vmin[q][d] += y1 * vj[q][d];
@@ -919,16 +920,16 @@ struct TeamChain {
     // the Chebyshev series) and D A (A = Fs + Fe, the predictor's force).
     // fuse: also form DX0 = D X0 and DA = D A in the start vector's pass;
     // otherwise the caller has them and the Lanczos forms D v0 itself.
-    __device__ void bounds(double* cache, int& cache_valid, double& lmin, double& lmax, const float (&X0)[2][3],
-                           const float (&A)[2][3], float (&DX0)[2][3], float (&DA)[2][3], bool fuse = true) {
-        double vmin[2][3], vmax[2][3], rmin, rmax;
+    __device__ void bounds(double* cache, int& cache_valid, double& lmin, double& lmax, const float (&X0)[Q][3],
+                           const float (&A)[Q][3], float (&DX0)[Q][3], float (&DA)[Q][3], bool fuse = true) {
+        double vmin[Q][3], vmax[Q][3], rmin, rmax;
         const bool can_warm = cache_valid != 0;
-        double v0[2][3], dv0[2][3];
+        double v0[Q][3], dv0[Q][3];
         start_vector(can_warm, cache, v0);
         if (fuse) {
-            float x3[3][2][3], y3[3][2][3];
+            float x3[3][Q][3], y3[3][Q][3];
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     x3[0][q][d] = (float)v0[q][d];
@@ -937,7 +938,7 @@ struct TeamChain {
                 }
             applyK<3>(x3, y3);
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     dv0[q][d] = (double)y3[0][q][d];
@@ -954,18 +955,18 @@ struct TeamChain {
         } else {
             cnt[can_warm ? C_LZWARM : C_LZCOLD] += 1;
         }
-        double s[2][3], u[2][3];
+        double s[Q][3], u[Q][3];
         load(a.seed_table, u);
         const double iun = 1.0 / ch.seed_norm;
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) s[q][d] = vmin[q][d] + vmax[q][d] + 0.01 * u[q][d] * iun;
         const double sn = sqrt(dot(s, s));
         if (sn > 0.0 && isfinite(sn)) {
             const double is = 1.0 / sn;
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) s[q][d] *= is;
             store(cache, s);
@@ -984,8 +985,8 @@ struct TeamChain {
     // Dx0 = D x0 (computed by the caller). grow: the FD growth loop of the
     // reference; without it a failed check returns at once (bounds kept from
     // an earlier step are refreshed first).
-    __device__ double chebyshev(const float (&x0)[2][3], const float (&Dx0)[2][3], double lmin, double lmax,
-                                float (&out)[2][3], bool grow = true) {
+    __device__ double chebyshev(const float (&x0)[Q][3], const float (&Dx0)[Q][3], double lmin, double lmax,
+                                float (&out)[Q][3], bool grow = true) {
         const double x0Dx0 = dotf(x0, Dx0);
         double Lr = sqrt(lmax / lmin) * ch.mult + 0.5;
         int L = !(Lr < 2.0e9) ? kMaxCheb : (int)Lr + 1;
@@ -1009,10 +1010,10 @@ struct TeamChain {
                 coef[j] = s;
             }
             sync();
-            float tp[2][3], tc[2][3], o[2][3];
+            float tp[Q][3], tc[Q][3], o[Q][3];
             const float c0 = coef[0], c1 = coef[1];
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     tp[q][d] = x0[q][d];
@@ -1020,11 +1021,11 @@ struct TeamChain {
                     o[q][d] = c0 * tp[q][d] + c1 * tc[q][d];
                 }
             for (int l = 2; l <= L; ++l) {
-                float Dv[2][3];
+                float Dv[Q][3];
                 apply32(tc, Dv);
                 const float cl = coef[l];
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
                         const float tn = 2.f * (da * Dv[q][d] + db * tc[q][d]) - tp[q][d];
@@ -1035,7 +1036,7 @@ struct TeamChain {
             }
             cnt[C_CHEB] += L;
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) out[q][d] = valid(q) ? o[q][d] : 0.f;
             const double rr = dotf(out, out);
@@ -1050,7 +1051,7 @@ struct TeamChain {
 
     // ---- Cholesky fallback (src/mobility.cpp:69-81): dense FP64 D in global
     // scratch, right-looking factor, L x0. Returns false if not PD.
-    __device__ bool cholesky_noise(const double (&R)[2][3], const float (&x0)[2][3], float (&out)[2][3]) {
+    __device__ bool cholesky_noise(const double (&R)[Q][3], const float (&x0)[Q][3], float (&out)[Q][3]) {
         to_smem(S.s0, R);
         sync();
         double* L = Lt;
@@ -1096,13 +1097,13 @@ struct TeamChain {
             sync();
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
             if (valid(q))
 #pragma unroll
                 for (int d = 0; d < 3; ++d) S.s1[3 * bead(q) + d] = (double)x0[q][d];
         sync();
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < Q; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 const int i = 3 * bead(q) + d;
@@ -1118,17 +1119,17 @@ struct TeamChain {
 
 // -------------------------------------------------------------- the kernel
 
-template <int T>
-__global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlocks)
+template <int T, int Q>
+__global__ void __launch_bounds__(TeamCfg<T, Q>::kCtaThreads, TeamCfg<T, Q>::kMinBlocks)
     integrate_team_kernel(const RunArgs a) {
     extern __shared__ __align__(16) unsigned char wsm[];
-    constexpr int TT = TeamCfg<T>::kThreads;
+    constexpr int TT = TeamCfg<T, Q>::kThreads;
     const int team = threadIdx.x / TT;
     const int tid = threadIdx.x % TT;
-    const int64_t stride = team_area_stride<T>(a.n_max);
-    TeamShared<T>& S = *reinterpret_cast<TeamShared<T>*>(wsm + stride * team);
-    double* Vs = reinterpret_cast<double*>(wsm + stride * team + (sizeof(TeamShared<T>) + 15) / 16 * 16);
-    const int64_t gw = (int64_t)blockIdx.x * TeamCfg<T>::kTeamsPerCta + team;
+    const int64_t stride = team_area_stride<T, Q>(a.n_max);
+    TeamShared<T, Q>& S = *reinterpret_cast<TeamShared<T, Q>*>(wsm + stride * team);
+    double* Vs = reinterpret_cast<double*>(wsm + stride * team + (sizeof(TeamShared<T, Q>) + 15) / 16 * 16);
+    const int64_t gw = (int64_t)blockIdx.x * TeamCfg<T, Q>::kTeamsPerCta + team;
     double* scr = a.scratch + gw * a.scratch_stride;
     const int nvr = (int)round_up8(a.n_max);
     const uint64_t t_launch = global_ns();
@@ -1155,7 +1156,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             team_sync<T>(team);
             continue;
         }
-        TeamChain<T> W(a, S, ch);
+        TeamChain<T, Q> W(a, S, ch);
         W.V = Vs;
         W.sqx = reinterpret_cast<float*>(Vs);
         W.coef = reinterpret_cast<float*>(Vs) + kCoefCap;
@@ -1188,7 +1189,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
         int cache_valid = (a.cache_mode == BDCU_CACHE_PERSIST) ? a.cache_valid[c] : 0;
         uint32_t ux = (uint32_t)a.rng[3 * c];
         int32_t iy = a.rng[3 * c + 1], seed = a.rng[3 * c + 2];
-        double R[2][3];
+        double R[Q][3];
         W.load(gR, R);
         const int nsteps = a.n_steps[c];
         double t = a.t_start[c];
@@ -1209,29 +1210,29 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                 for (int d = 0; d < 3; ++d) {
                     double s = 0.0;
 #pragma unroll
-                    for (int q = 0; q < 2; ++q) s += R[q][d];
+                    for (int q = 0; q < Q; ++q) s += R[q][d];
                     com[d] = (1.0 / N) * W.tsum(s);
                 }
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
                     if (W.valid(q))
                         for (int d = 0; d < 3; ++d) R[q][d] -= com[d];
             }
             W.stage_pos(R);
-            float Fs[2][3], Fe[2][3];
+            float Fs[Q][3], Fe[Q][3];
             W.forces(R, t, Fs, Fe, true);
-            float X0[2][3], dW[2][3], A[2][3], DF[2][3];
+            float X0[Q][3], dW[Q][3], A[Q][3], DF[Q][3];
             W.noise(ux, iy, seed, X0);
             // brownian_step (src/mobility.cpp:58-88)
             if (!W.hi) {
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) dW[q][d] = (float)(sqrt_dt * X0[q][d]);
             } else {
-                float bx[2][3], DX0[2][3];
+                float bx[Q][3], DX0[Q][3];
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) A[q][d] = Fs[q][d] + Fe[q][d];
                 double fd;
@@ -1241,9 +1242,9 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                     fd = W.chebyshev(X0, DX0, lmin, lmax, bx);
                 } else {
                     // bounds kept from an earlier step: the two products in one pass
-                    float x2[2][2][3], y2[2][2][3];
+                    float x2[2][Q][3], y2[2][Q][3];
 #pragma unroll
-                    for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < Q; ++q)
 #pragma unroll
                         for (int d = 0; d < 3; ++d) {
                             x2[0][q][d] = X0[q][d];
@@ -1251,7 +1252,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                         }
                     W.template applyK<2>(x2, y2);
 #pragma unroll
-                    for (int q = 0; q < 2; ++q)
+                    for (int q = 0; q < Q; ++q)
 #pragma unroll
                         for (int d = 0; d < 3; ++d) {
                             DX0[q][d] = y2[0][q][d];
@@ -1274,7 +1275,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) dW[q][d] = (float)(sqrt_dt * bx[q][d]);
             }
@@ -1282,14 +1283,14 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             double K1[9], K2[9];
             kappa_at(ch, a.arena, t, K1);
             kappa_at(ch, a.arena, t + dt, K2);
-            double Rp[2][3];
+            double Rp[Q][3];
             if (!W.hi)  // without HI D = I; with HI, bounds() formed D (Fs + Fe)
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) DF[q][d] = Fs[q][d] + Fe[q][d];
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
                     const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
@@ -1297,16 +1298,16 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                 }
             // upsilon (src/integrator.cpp:107-119): forces at R~ with R~'s coordinates staged
             W.stage_pos(Rp);
-            float Fep[2][3], dummy[2][3];
+            float Fep[Q][3], dummy[Q][3];
             W.forces(Rp, t + dt, dummy, Fep, false);
             // D Fs + D (Fe + Fe~) = D (Fs + Fe) + D Fe~: the predictor's
             // product plus one more (the reference forms both sums anew)
             W.stage_pos(R);
-            float DFep[2][3];
-            double ups[2][3];
+            float DFep[Q][3];
+            double ups[Q][3];
             W.applyF(Fep, DFep);
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
                     const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
@@ -1318,9 +1319,9 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             W.to_smem(S.s0, ups);
             W.to_smem(S.s1, Rp);
             team_sync<T>(team);
-            double dups[2][3], bond[2][3];
+            double dups[Q][3], bond[Q][3];
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 const int b = W.bead(q);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -1331,9 +1332,9 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             }
             const double anchor0 = S.s1[0], anchor1 = S.s1[1], anchor2 = S.s1[2];
             team_sync<T>(team);
-            double Rprev[2][3], Rc[2][3];
+            double Rprev[Q][3], Rc[Q][3];
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) Rprev[q][d] = Rp[q][d];
             const int max_iter = 100 * N;
@@ -1341,9 +1342,9 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             int lstat = 0;
             for (int iter = 0;; ++iter) {
                 // connector forces (src/spring.cpp:183-193) into s1, bead forces
-                double Fc[2][3];
+                double Fc[Q][3];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
+                for (int q = 0; q < Q; ++q) {
                     const int b = W.bead(q);
                     const double f =
                         b < N - 1 ? connector_factor(ch, clamped_len(bond[q][0], bond[q][1], bond[q][2])) : 0.0;
@@ -1354,9 +1355,9 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                     }
                 }
                 team_sync<T>(team);
-                float Fb[2][3], DFb[2][3];
+                float Fb[Q][3], DFb[Q][3];
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
+                for (int q = 0; q < Q; ++q) {
                     const int m = W.bead(q);
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
@@ -1372,13 +1373,13 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                 team_sync<T>(team);
                 W.applyF(Fb, DFb);
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
                     if (W.valid(q))
 #pragma unroll
                         for (int d = 0; d < 3; ++d) S.s2[3 * W.bead(q) + d] = (double)DFb[q][d];
                 team_sync<T>(team);
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
+                for (int q = 0; q < Q; ++q) {
                     const int b = W.bead(q);
                     if (b < N - 1) {
                         double g[3], qv[3];
@@ -1391,30 +1392,33 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                 // R_corr = anchor + prefix sums of the bonds: inclusive scan in
                 // each warp, then the totals of the warps before it (slot 0 of
                 // the whole team precedes slot 1)
-                double scan[2][3];
+                double scan[Q][3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    double v0 = bond[0][d], v1 = bond[1][d];
+                    double v[Q];
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) v[q] = bond[q][d];
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
-                        const double t0 = __shfl_up_sync(kFull, v0, o);
-                        const double t1 = __shfl_up_sync(kFull, v1, o);
-                        if (W.wl >= o) {
-                            v0 += t0;
-                            v1 += t1;
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) {
+                            const double tq = __shfl_up_sync(kFull, v[q], o);
+                            if (W.wl >= o) v[q] += tq;
                         }
                     }
-                    scan[0][d] = v0;
-                    scan[1][d] = v1;
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) scan[q][d] = v[q];
                 }
                 if constexpr (T == 1) {
+                    if constexpr (Q == 2) {
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) scan[1][d] += __shfl_sync(kFull, scan[0][d], 31);
+                        for (int d = 0; d < 3; ++d) scan[1][d] += __shfl_sync(kFull, scan[0][d], 31);
+                    }
                     __syncwarp();
                 } else {
                     if (W.wl == 31)
 #pragma unroll
-                        for (int q = 0; q < 2; ++q)
+                        for (int q = 0; q < Q; ++q)
 #pragma unroll
                             for (int d = 0; d < 3; ++d) S.tot[(q * 3 + d) * T + W.wi] = scan[q][d];
                     team_sync<T>(team);
@@ -1423,7 +1427,8 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                         double off0 = 0.0, all0 = 0.0, off1 = 0.0;
 #pragma unroll
                         for (int w = 0; w < T; ++w) {
-                            const double t0 = S.tot[d * T + w], t1 = S.tot[(3 + d) * T + w];
+                            const double t0 = S.tot[d * T + w];
+                            const double t1 = Q == 2 ? S.tot[(3 + d) * T + w] : 0.0;
                             if (w < W.wi) {
                                 off0 += t0;
                                 off1 += t1;
@@ -1431,7 +1436,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                             all0 += t0;
                         }
                         scan[0][d] += off0;
-                        scan[1][d] += all0 + off1;
+                        if constexpr (Q == 2) scan[1][d] += all0 + off1;
                     }
                 }
                 team_sync<T>(team);
@@ -1442,7 +1447,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                 }
                 const double an[3] = {anchor0, anchor1, anchor2};
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
+                for (int q = 0; q < Q; ++q) {
                     const int b = W.bead(q);
                     if (b < N - 1)
                         for (int d = 0; d < 3; ++d) S.s1[3 * (b + 1) + d] = an[d] + scan[q][d];
@@ -1452,7 +1457,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                 team_sync<T>(team);
                 double s = 0.0;
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
                     if (W.valid(q)) {
                         const double e0 = Rc[q][0] - Rprev[q][0], e1 = Rc[q][1] - Rprev[q][1],
                                      e2 = Rc[q][2] - Rprev[q][2];
@@ -1471,7 +1476,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
                     break;
                 }
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
+                for (int q = 0; q < Q; ++q)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) Rprev[q][d] = Rc[q][d];
             }
@@ -1479,7 +1484,7 @@ __global__ void __launch_bounds__(TeamCfg<T>::kCtaThreads, TeamCfg<T>::kMinBlock
             W.status |= W.tor(lstat);
             if (W.status & BDCU_ST_FATAL_MASK) break;
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
+            for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) R[q][d] = Rc[q][d];
             W.cnt[C_STEPS] += 1;

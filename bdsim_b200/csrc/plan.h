@@ -22,18 +22,35 @@ inline int bucket_of(const DevChain& c, int form) {
     return kMaxBuckets - 1;
 }
 
-inline int64_t team_smem(int T, int n_max) {
-    switch (T) {
-        case 1: return team_smem_bytes<1>(n_max);
-        case 2: return team_smem_bytes<2>(n_max);
-        case 4: return team_smem_bytes<4>(n_max);
-        default: return team_smem_bytes<8>(n_max);
-    }
+#define BDCU_TEAM_SHAPE_SWITCH(T, Q, EXPR, FALLBACK)            \
+    (T == 1 && Q == 2)   ? EXPR(1, 2)                            \
+    : (T == 2 && Q == 1) ? EXPR(2, 1)                            \
+    : (T == 2 && Q == 2) ? EXPR(2, 2)                            \
+    : (T == 4 && Q == 1) ? EXPR(4, 1)                            \
+    : (T == 4 && Q == 2) ? EXPR(4, 2)                            \
+    : (T == 8 && Q == 1) ? EXPR(8, 1)                            \
+    : (T == 8 && Q == 2) ? EXPR(8, 2)                            \
+                         : FALLBACK
+
+// Shared memory of a team-kernel block of shape (T, Q) for chains of up to
+// n_max/3 beads (-1: no such shape).
+inline int64_t team_smem(int T, int Q, int n_max) {
+#define BDCU_SMEM(t, q) team_smem_bytes<t, q>(n_max)
+    return BDCU_TEAM_SHAPE_SWITCH(T, Q, BDCU_SMEM, (int64_t)-1);
+#undef BDCU_SMEM
 }
 
-inline int teams_per_cta(int T) {
-    return T == 1 ? TeamCfg<1>::kTeamsPerCta : T == 2 ? TeamCfg<2>::kTeamsPerCta
-         : T == 4 ? TeamCfg<4>::kTeamsPerCta : TeamCfg<8>::kTeamsPerCta;
+inline int teams_per_cta(int T, int Q) {
+#define BDCU_TPC(t, q) TeamCfg<t, q>::kTeamsPerCta
+    return BDCU_TEAM_SHAPE_SWITCH(T, Q, BDCU_TPC, 1);
+#undef BDCU_TPC
+}
+
+// Whether (T, Q) is a compiled team shape that holds chains of `beads`.
+inline bool team_shape_fits(int T, int Q, int beads) {
+    for (int i = 0; i < kNumTeamShapes; ++i)
+        if (kTeamShapes[i][0] == T && kTeamShapes[i][1] == Q) return beads <= 32 * T * Q;
+    return false;
 }
 
 // Threads per block of the block kernel's heuristic shape: one thread per row

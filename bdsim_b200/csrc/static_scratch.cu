@@ -40,8 +40,8 @@ cudaError_t launch_plain(const RunArgs& a, int grid, int block, size_t smem, cud
 cudaError_t launch_mixed(const RunArgs& a, int grid, int block, size_t smem, cudaStream_t s);
 cudaError_t occupancy_plain(int block, size_t smem, int* per_sm);
 cudaError_t occupancy_mixed(int block, size_t smem, int* per_sm);
-cudaError_t launch_mixed_team(int team_warps, const RunArgs& a, int grid, size_t smem, cudaStream_t s);
-cudaError_t occupancy_mixed_team(int team_warps, size_t smem, int* per_sm);
+cudaError_t launch_mixed_team(int team_warps, int team_q, const RunArgs& a, int grid, size_t smem, cudaStream_t s);
+cudaError_t occupancy_mixed_team(int team_warps, int team_q, size_t smem, int* per_sm);
 DevChain derive_record(const bdcu_phys& p, const bdcu_sim& s, int64_t bead_off);
 int validate_chain(bdcu_ctx* ctx, int i, const bdcu_phys& p, const bdcu_sim& s, const double* arena,
                    int64_t arena_len);
@@ -171,13 +171,13 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
         if (id < kFirstBlockBucket) {
             any_team = true;
             l.team_warps = 1 << id;
-            l.smem = (size_t)team_smem(l.team_warps, l.n_max);
+            l.smem = (size_t)team_smem(l.team_warps, 2, l.n_max);
             if (l.smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: team kernel shared memory too large");
-            e = occupancy_mixed_team(l.team_warps, l.smem, &per_sm);
+            e = occupancy_mixed_team(l.team_warps, 2, l.smem, &per_sm);
             l.stride = l.need_d ? team_scratch_doubles(l.n_max) : 1;
-            l.per_block = sizeof(double) * (size_t)l.stride * teams_per_cta(l.team_warps);
-            l.block = 32 * l.team_warps * teams_per_cta(l.team_warps);
-            l.grid = (l.count + teams_per_cta(l.team_warps) - 1) / teams_per_cta(l.team_warps);
+            l.per_block = sizeof(double) * (size_t)l.stride * teams_per_cta(l.team_warps, 2);
+            l.block = 32 * l.team_warps * teams_per_cta(l.team_warps, 2);
+            l.grid = (l.count + teams_per_cta(l.team_warps, 2) - 1) / teams_per_cta(l.team_warps, 2);
         } else {
             std::vector<int> d_opts = (!mixed && l.need_d) ? std::vector<int>{1, 0} : std::vector<int>{0};
             std::vector<int> v_opts = l.need_lz ? std::vector<int>{kLanczosCold, kLanczosWarm, 0} : std::vector<int>{0};
@@ -293,7 +293,7 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
         a.xs_pow = reinterpret_cast<const uint32_t*>(b + o_cols);
         a.a_pow = reinterpret_cast<const uint32_t*>(b + o_apow);
         if (l.id < kFirstBlockBucket)
-            e = launch_mixed_team(l.team_warps, a, l.grid, l.smem, s);
+            e = launch_mixed_team(l.team_warps, 2, a, l.grid, l.smem, s);
         else
             e = mixed ? launch_mixed(a, l.grid, l.block, l.smem, s) : launch_plain(a, l.grid, l.block, l.smem, s);
         if (e != cudaSuccess)

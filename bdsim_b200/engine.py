@@ -144,6 +144,12 @@ class Context:
                                         dptr(cache_valid), dptr(t_start), int(probe_steps)), "bdcu_autotune")
         return self.describe_plan(form)
 
+    def set_team_shape(self, bucket: int, team_warps: int, beads_per_thread: int = 2):
+        """Pin the FP32-mixed form's team shape for team bucket 0..3 (warps
+        per chain, beads per thread); team_warps=0 restores the default."""
+        self._ck(self.lib.bdcu_set_team_shape(self.h, int(bucket), int(team_warps), int(beads_per_thread)),
+                 "bdcu_set_team_shape")
+
     # ---- slot pools (serving)
 
     def reserve(self, n_slots: int, bead_capacity: int, arena_len: int = 0):

@@ -290,22 +290,35 @@ typedef struct bdcu_bucket_info {
     int32_t v_cap;       /* Lanczos basis vectors kept in shared memory */
     int32_t d_in_smem;   /* dense D in shared memory (plain form) */
     int32_t tuned;       /* 1: shape chosen by bdcu_autotune */
-    int32_t reserved;
+    int32_t team_beads_per_thread;  /* team kernel: 1 or 2 beads per thread (0 for the block kernel) */
     int64_t smem_bytes;  /* dynamic shared memory per block */
 } bdcu_bucket_info;
 /* The plan bdcu_run would use for `form` on the current selection; writes up
    to `cap` buckets (cap >= BDCU_MAX_BUCKETS always suffices) and their count. */
 int bdcu_describe_plan(bdcu_ctx* ctx, int form, bdcu_bucket_info* out, int cap, int* n_out);
 
-/* Time every launch shape of each block-kernel bucket of the current selection
-   (threads per block x Lanczos vectors in shared memory x, in the plain form,
-   D in shared memory) for probe_steps steps on device copies of the given state
-   -- the caller's buffers are read, never written -- and keep the fastest shape
-   per (form, bucket) for later bdcu_run calls. Synchronous; allocates and frees
-   its copies. The shape changes only the speed and, through block reductions,
-   the rounding of the Lanczos and Chebyshev dot products. */
+/* Time every launch shape of each bucket of the current selection for
+   probe_steps steps on device copies of the given state -- the caller's buffers
+   are read, never written -- and keep the fastest shape per (form, bucket) for
+   later bdcu_run calls. Block-kernel buckets: threads per block x Lanczos
+   vectors in shared memory x, in the plain form, D in shared memory.
+   Team-kernel buckets (FP32-mixed form): warps per team x beads per thread,
+   every compiled team shape that holds any chain of the bucket, up to twice
+   its width. No
+   counterpart in the reference (one chain per call on the CPU). Synchronous;
+   allocates and frees its copies. The shape changes only the speed and,
+   through the order of block and team reductions, the rounding of the
+   Lanczos and Chebyshev dot products. */
 int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, const double* cache,
                   const int32_t* cache_valid, const double* t_start, int probe_steps);
+
+/* Pin the team shape of team-kernel bucket `bucket` (0..3) of the FP32-mixed
+   form: team_warps warps per chain with beads_per_thread (1 or 2) beads per
+   thread, a compiled shape that holds every chain the bucket admits (32 *
+   team_warps * beads_per_thread >= 64, 128, 256, 512 for buckets 0..3). team_warps = 0 returns the bucket to
+   the default shape. Later bdcu_autotune calls replace it. No counterpart in
+   the reference. */
+int bdcu_set_team_shape(bdcu_ctx* ctx, int bucket, int team_warps, int beads_per_thread);
 
 /* ---- Slot pools, for a serving loop that admits and retires chains between
    runs (no counterpart in the reference).

@@ -105,7 +105,7 @@ def test_uneven_batch_mixed_matches_oracle_and_alone(uneven, port_results):
 
 
 @pytest.mark.parametrize("form", ["plain", "mixed"])
-def test_autotune_leaves_state_and_tunes_every_block_bucket(uneven, port_results, form):
+def test_autotune_leaves_state_and_tunes_every_bucket(uneven, port_results, form):
     import torch
     ens = _ensemble(uneven, form)
     R0 = ens.R.clone()
@@ -114,7 +114,7 @@ def test_autotune_leaves_state_and_tunes_every_block_bucket(uneven, port_results
     torch.cuda.synchronize()
     assert torch.equal(ens.R, R0) and torch.equal(ens.rng, rng0)
     for b in plan:
-        assert b["tuned"] == (1 if b["kernel"] == _abi.KERNEL_BLOCK else 0), b
+        assert b["tuned"] == 1, b  # block-kernel buckets and (mixed form) team buckets
     ens.advance(0.0, STEPS, _abi.CACHE_RESET_PER_CALL)
     got = ens.positions()
     tol = CALL_TOL if form == "plain" else MIXED_TOL
@@ -217,3 +217,40 @@ def test_graph_capture_replays_an_uneven_run(uneven):
     assert torch.equal(a.R, b.R) and torch.equal(a.rng, b.rng) and torch.equal(a.cache, b.cache)
     assert torch.equal(a.counters, b.counters)
     del g
+
+
+# team shapes (warps per chain, beads per thread) compiled into the library
+TEAM_SHAPES = [(1, 2), (2, 1), (2, 2), (4, 1), (4, 2), (8, 1), (8, 2)]
+BUCKET_BEADS = [64, 128, 256, 512]
+
+
+@pytest.mark.parametrize("bucket", [0, 1, 2, 3])
+def test_every_team_shape_matches_oracle(uneven, port_results, bucket):
+    """Each team shape that holds a bucket (up to twice its width) gives the
+    reference's RNG stream and stays within MIXED_TOL of the oracle."""
+    phys, sims, R0, seeds = uneven
+    shapes = [(T, Q) for T, Q in TEAM_SHAPES
+              if BUCKET_BEADS[bucket] <= 32 * T * Q <= 2 * BUCKET_BEADS[bucket]]
+    assert shapes  # bucket 3 (N <= 512) has one shape, (8, 2)
+    for T, Q in shapes:
+        ens = _ensemble(uneven, "mixed")
+        ens.ctx.set_team_shape(bucket, T, Q)
+        b = {x["bucket"]: x for x in ens.plan()}[bucket]
+        assert (b["team_warps"], b["team_beads_per_thread"], b["tuned"]) == (T, Q, 1), b
+        ens.advance(0.0, STEPS, _abi.CACHE_RESET_PER_CALL)
+        got = ens.positions()
+        states = ens.rng_states()
+        for i, (R, st, _) in enumerate(port_results):
+            assert states[i] == st, (T, Q, i)
+            assert rel(got[i], R) <= MIXED_TOL, (T, Q, NS[i], rel(got[i], R))
+
+
+def test_team_shape_rejects_a_shape_that_does_not_hold_the_bucket(uneven):
+    ens = _ensemble(uneven, "mixed")
+    with pytest.raises(BdcuError):
+        ens.ctx.set_team_shape(0, 3, 1)
+    with pytest.raises(BdcuError):
+        ens.ctx.set_team_shape(2, 2, 1)  # compiled, but 64 beads cannot hold bucket 2 (N <= 256)
+    ens.ctx.set_team_shape(2, 4, 1)
+    ens.ctx.set_team_shape(2, 0, 0)  # back to the default
+    assert {x["bucket"]: x for x in ens.plan()}[2]["team_warps"] == 4
