@@ -351,82 +351,147 @@ struct TeamChain {
     }
 
     // ---- FP32 matrix-free D.x (Diffusion::apply, src/mobility.cpp:53-56;
-    // RPY weights src/hydrodynamics.cpp:36-43). x, y: the thread's two beads.
+    // RPY weights src/hydrodynamics.cpp:36-43). x, y: the thread's beads.
     // K products against the same D in one pass over the bead pairs: the
     // pair geometry and weights are computed once for all K inputs (K = 3
     // for the products of a step that do not depend on one another).
-    // Inputs are staged in S.xs and, for K > 1, in S.s1 / S.s2 viewed as
-    // float4 (free while the mobility products run).
+    //
+    // The single products (K = 1, most of the step's passes) take the
+    // partner beads j two at a time in packed FP32x2 arithmetic (sm_100's
+    // FADD2 / FMUL2 / FFMA2: one issue slot for the pair; the FP32 pipe rate
+    // is that of scalar FFMA, measured 73 TFLOP/s on one B200 either way),
+    // from coordinates and inputs staged by component in shared memory, so
+    // one 64-bit broadcast load brings (j, j+1) of a component. Each bead's
+    // sum is kept as two interleaved partial sums (even and odd j), added at
+    // the end. An odd N is padded with one zero input (whose contribution
+    // om1 * 0 + om2 (d . 0) d is exactly zero).
     template <int K>
     __device__ void applyK(const float (&x)[K][Q][3], float (&acc)[K][Q][3]) {
         static_assert(K >= 1 && K <= 3, "applyK stages at most three inputs");
-        using Shared = TeamShared<T, Q>;
-        static_assert(offsetof(Shared, s1) % 16 == 0 && offsetof(Shared, s2) % 16 == 0 &&
-                          sizeof(Shared::s1) >= sizeof(float4) * 32 * T * Q,
-                      "s1 / s2 must hold a 16-byte aligned float4 per bead");
         cnt[C_DX] += K;
-        float4* stage[3] = {S.xs, reinterpret_cast<float4*>(S.s1), reinterpret_cast<float4*>(S.s2)};
 #pragma unroll
         for (int q = 0; q < Q; ++q)
             if (valid(q))
 #pragma unroll
-                for (int r = 0; r < K; ++r) stage[r][bead(q)] = make_float4(x[r][q][0], x[r][q][1], x[r][q][2], 0.f);
+                for (int r = 0; r < K; ++r)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) S.xk[r][d][bead(q)] = x[r][q][d];
+        if ((N & 1) && tid < 3 * K) S.xk[tid / 3][tid % 3][N] = 0.f;
         sync();
-        float4 pb[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            pb[q] = valid(q) ? S.pos[bead(q)] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int r = 0; r < K; ++r)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
-        }
         // In units of h*: with d = (R_j - R_b)/h*, s = |d|^2, rho = s^-1/2,
         //   far  (s >= 4 pi): om1 = rho (K1 + K2 rho^2), om2 = rho^3 (K1 - K3 rho^2)
         //   near (s <  4 pi): om1 = 1 - C3 s rho,         om2 = C7 rho
-        // and y_b += om1 x_j + om2 (d.x_j) d. The self pair (d = 0, s clamped
-        // to 1e-24) takes the near branch with om1 = 1 exactly in FP32 and
-        // om2 d = 0: it contributes the identity block.
+        // and y_b += om1 x_j + om2 (d.x_j) d, with the branch folded into
+        // selected factors, om1 = B U + A and om2 = P V (selects run on the
+        // integer pipe, the FP32 pipe does one FFMA and one FMUL). The self
+        // pair (d = 0, s clamped to 1e-24) takes the near branch with om1 = 1
+        // exactly in FP32 and om2 d = 0: it contributes the identity block.
         bool one_slot = false;
         if constexpr (T > 1 && Q == 2) one_slot = __all_sync(kFull, !valid(1));
         const int nq = one_slot ? 1 : Q;
-        // not unrolled: this loop is inlined at every product's call site, and
-        // the smaller code measured 6% faster on the 4096 x N=50 workload
-        // (fewer instruction-fetch stalls) despite a few more register spills
+        if constexpr (K == 1) {
+            // the Lanczos, Chebyshev, upsilon and corrector products: partner
+            // beads two at a time in packed FP32x2
+            float2 nb[Q][3], a[Q][3];
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const float v = valid(q) ? -S.ps[d][bead(q)] : 0.f;
+                    nb[q][d] = make_float2(v, v);
+                    a[q][d] = make_float2(0.f, 0.f);
+                }
+            const float2 k1 = make_float2(K1, K1), k2 = make_float2(K2, K2), mk3 = make_float2(-K3, -K3);
+            const int n2 = (N + 1) & ~1;
+            // not unrolled: this loop is inlined at every product's call site
 #pragma unroll 1
-        for (int j = 0; j < N; ++j) {
-            const float4 pj = S.pos[j];
-            float4 xj[K];
+            for (int j = 0; j < n2; j += 2) {
+                float2 pj[3], xj[3];
 #pragma unroll
-            for (int r = 0; r < K; ++r) xj[r] = stage[r][j];
+                for (int d = 0; d < 3; ++d) {
+                    pj[d] = *reinterpret_cast<const float2*>(&S.ps[d][j]);
+                    xj[d] = *reinterpret_cast<const float2*>(&S.xk[0][d][j]);
+                }
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                if (q < nq) {
-                    const float dx = pj.x - pb[q].x, dy = pj.y - pb[q].y, dz = pj.z - pb[q].z;
-                    const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
-                    const float rho = rsqrtf(sq);
-                    const float rho2 = rho * rho;
-                    const bool far = sq >= 12.566370614359172f;
-                    const float om1 = far ? rho * (K1 + K2 * rho2) : 1.f - C3 * (sq * rho);
-                    const float om2 = far ? (rho * rho2) * (K1 - K3 * rho2) : C7 * rho;
-#pragma unroll
-                    for (int r = 0; r < K; ++r) {
-                        const float tt = om2 * (dx * xj[r].x + dy * xj[r].y + dz * xj[r].z);
-                        acc[r][q][0] += om1 * xj[r].x + tt * dx;
-                        acc[r][q][1] += om1 * xj[r].y + tt * dy;
-                        acc[r][q][2] += om1 * xj[r].z + tt * dz;
+                for (int q = 0; q < Q; ++q) {
+                    if (q < nq) {
+                        const float2 dx = __fadd2_rn(pj[0], nb[q][0]);
+                        const float2 dy = __fadd2_rn(pj[1], nb[q][1]);
+                        const float2 dz = __fadd2_rn(pj[2], nb[q][2]);
+                        float2 sq = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                        sq = make_float2(fmaxf(sq.x, 1e-24f), fmaxf(sq.y, 1e-24f));
+                        const float2 rho = make_float2(rsqrtf(sq.x), rsqrtf(sq.y));
+                        const float2 t = __fmul2_rn(rho, rho);
+                        const float2 u = __ffma2_rn(k2, t, k1), v = __ffma2_rn(mk3, t, k1);
+                        const float2 r = __fmul2_rn(sq, rho), rt = __fmul2_rn(rho, t);
+                        const bool fx = sq.x >= 12.566370614359172f, fy = sq.y >= 12.566370614359172f;
+                        const float2 om1 = __ffma2_rn(make_float2(fx ? rho.x : -C3, fy ? rho.y : -C3),
+                                                      make_float2(fx ? u.x : r.x, fy ? u.y : r.y),
+                                                      make_float2(fx ? 0.f : 1.f, fy ? 0.f : 1.f));
+                        const float2 om2 = __fmul2_rn(make_float2(fx ? rt.x : C7, fy ? rt.y : C7),
+                                                      make_float2(fx ? v.x : rho.x, fy ? v.y : rho.y));
+                        const float2 tt =
+                            __fmul2_rn(om2, __ffma2_rn(dz, xj[2], __ffma2_rn(dy, xj[1], __fmul2_rn(dx, xj[0]))));
+                        a[q][0] = __ffma2_rn(tt, dx, __ffma2_rn(om1, xj[0], a[q][0]));
+                        a[q][1] = __ffma2_rn(tt, dy, __ffma2_rn(om1, xj[1], a[q][1]));
+                        a[q][2] = __ffma2_rn(tt, dz, __ffma2_rn(om1, xj[2], a[q][2]));
                     }
                 }
             }
-        }
-        sync();
+            sync();
 #pragma unroll
-        for (int q = 0; q < Q; ++q)
-            if (!valid(q))
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) acc[0][q][d] = valid(q) ? a[q][d].x + a[q][d].y : 0.f;
+        } else {
+            // the fused products of a step (K = 2, 3), once or twice per
+            // step: scalar FP32, fewer live registers than the packed form
+            float pb[Q][3];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) pb[q][d] = valid(q) ? S.ps[d][bead(q)] : 0.f;
 #pragma unroll
                 for (int r = 0; r < K; ++r)
 #pragma unroll
                     for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
+            }
+#pragma unroll 1
+            for (int j = 0; j < N; ++j) {
+                const float px = S.ps[0][j], py = S.ps[1][j], pz = S.ps[2][j];
+                float xj[K][3];
+#pragma unroll
+                for (int r = 0; r < K; ++r)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) xj[r][d] = S.xk[r][d][j];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    if (q < nq) {
+                        const float dx = px - pb[q][0], dy = py - pb[q][1], dz = pz - pb[q][2];
+                        const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
+                        const float rho = rsqrtf(sq), t = rho * rho;
+                        const bool far = sq >= 12.566370614359172f;
+                        const float om1 = fmaf(far ? rho : -C3, far ? fmaf(K2, t, K1) : sq * rho, far ? 0.f : 1.f);
+                        const float om2 = (far ? rho * t : C7) * (far ? fmaf(-K3, t, K1) : rho);
+#pragma unroll
+                        for (int r = 0; r < K; ++r) {
+                            const float tt = om2 * (dx * xj[r][0] + dy * xj[r][1] + dz * xj[r][2]);
+                            acc[r][q][0] += om1 * xj[r][0] + tt * dx;
+                            acc[r][q][1] += om1 * xj[r][1] + tt * dy;
+                            acc[r][q][2] += om1 * xj[r][2] + tt * dz;
+                        }
+                    }
+                }
+            }
+            sync();
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (!valid(q))
+#pragma unroll
+                    for (int r = 0; r < K; ++r)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
+        }
     }
 
     __device__ void apply32(const float (&x)[Q][3], float (&acc)[Q][3]) {
@@ -487,9 +552,14 @@ struct TeamChain {
         sync();
 #pragma unroll
         for (int q = 0; q < Q; ++q)
-            if (valid(q))
-                S.pos[bead(q)] = make_float4((float)(R[q][0] * iscale), (float)(R[q][1] * iscale),
-                                             (float)(R[q][2] * iscale), 0.f);
+            if (valid(q)) {
+                const float x = (float)(R[q][0] * iscale), y = (float)(R[q][1] * iscale), z = (float)(R[q][2] * iscale);
+                S.pos[bead(q)] = make_float4(x, y, z, 0.f);
+                S.ps[0][bead(q)] = x;
+                S.ps[1][bead(q)] = y;
+                S.ps[2][bead(q)] = z;
+            }
+        if ((N & 1) && tid < 3) S.ps[tid][N] = 0.f;  // the odd-N pad bead (zero input in every pass)
         sync();
     }
 

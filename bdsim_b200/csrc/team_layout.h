@@ -38,7 +38,8 @@ struct TeamCfg {
 template <int T, int Q>
 struct TeamShared {
     float4 pos[32 * T * Q];   // FP32 bead coordinates of the tensor's configuration
-    float4 xs[32 * T * Q];    // FP32 staged D.x input
+    float ps[3][32 * T * Q];  // the same coordinates by component (x, y, z rows), for the D.x pass
+    float xk[3][3][32 * T * Q];  // staged D.x inputs: product r, component d, bead
     double s0[96 * T * Q];    // FP64 neighbour-exchange buffers
     double s1[96 * T * Q];
     double s2[96 * T * Q];

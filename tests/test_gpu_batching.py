@@ -251,6 +251,6 @@ def test_team_shape_rejects_a_shape_that_does_not_hold_the_bucket(uneven):
         ens.ctx.set_team_shape(0, 3, 1)
     with pytest.raises(BdcuError):
         ens.ctx.set_team_shape(2, 2, 1)  # compiled, but 64 beads cannot hold bucket 2 (N <= 256)
-    ens.ctx.set_team_shape(2, 4, 1)
+    ens.ctx.set_team_shape(2, 8, 1)
     ens.ctx.set_team_shape(2, 0, 0)  # back to the default
     assert {x["bucket"]: x for x in ens.plan()}[2]["team_warps"] == 4
