@@ -83,12 +83,14 @@ struct ScratchLayout {
 };
 __host__ __device__ inline ScratchLayout scratch_layout(int n_max, int d_in_smem, int v_cap, int need_chol,
                                                         int mixed, int need_d, int need_lz) {
+    // every region a whole number of 128-byte lines (16 doubles), so that a
+    // block's D and factor start on a line of their own (discard.global.L2)
     ScratchLayout s;
     int64_t o = 0;
-    const int64_t nn = (int64_t)n_max * n_max;
-    s.D = o;  if (!mixed && need_d && !d_in_smem) o += nn;
-    s.Lt = o; if (need_chol) o += nn;
-    s.V = o;  if (need_lz && v_cap < kLanczosCold) o += (int64_t)kLanczosCold * round_up8(n_max);
+    const int64_t nn = (int64_t)n_max * n_max, nn16 = (nn + 15) / 16 * 16;
+    s.D = o;  if (!mixed && need_d && !d_in_smem) o += nn16;
+    s.Lt = o; if (need_chol) o += nn16;
+    s.V = o;  if (need_lz && v_cap < kLanczosCold) o += ((int64_t)kLanczosCold * round_up8(n_max) + 15) / 16 * 16;
     s.total = o;
     return s;
 }
@@ -118,6 +120,43 @@ static __device__ double block_dot(const double* a, const double* b, int n, doub
     }
     __syncthreads();
     return red[0] + red[1];
+}
+
+// y_r = D x_r for K vectors in one read of D: one row per thread, each
+// product summed over j in order exactly as matvec does
+// (src/linalg.cpp:81-89), so every y_r equals its own single product bit for
+// bit. The plain form reads D (L2-resident) once for the step's K mutually
+// independent products instead of K times.
+template <int K>
+__device__ __forceinline__ void matvec_dense_k(const double* __restrict__ D, int ld, const double* const (&x)[K],
+                                               double* const (&y)[K], int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s[K];
+#pragma unroll
+        for (int r = 0; r < K; ++r) s[r] = 0.0;
+        const double* col = D + i;
+#pragma unroll 4
+        for (int j = 0; j < n; ++j) {
+            const double d = col[(int64_t)j * ld];
+#pragma unroll
+            for (int r = 0; r < K; ++r) s[r] += d * x[r][j];
+        }
+#pragma unroll
+        for (int r = 0; r < K; ++r) y[r][i] = s[r];
+    }
+}
+
+// Drop the L2 lines of [p, p + doubles) without writing them back: the dense
+// D (and a factor) are rebuilt every step, so after a step's last read the
+// data is dead. p must start a 128-byte line and the range must end at the
+// end of its allocation's last line (scratch_layout rounds every region to
+// whole lines); a misaligned p is left alone.
+__device__ __forceinline__ void discard_l2(const double* p, int64_t doubles) {
+    if ((reinterpret_cast<uintptr_t>(p) & 127) != 0) return;
+    const int64_t lines = (doubles * 8 + 127) / 128;
+    const char* base = reinterpret_cast<const char*>(p);
+    for (int64_t l = threadIdx.x; l < lines; l += blockDim.x)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(base + 128 * l) : "memory");
 }
 
 // y = D x, one row per thread, summed over j in order (matvec,
@@ -266,6 +305,41 @@ struct Block {
             matvec_dense(D, ldd, x, y, n);
         } else {
             apply_D_pairwise(x, y);
+        }
+    }
+
+    // K products against D at once (K = 1..4): the plain form reads D once,
+    // the mixed form runs its matrix-free products one after another. Caller
+    // syncs before and after, as for apply_D.
+    template <int K>
+    __device__ void apply_D_multi(const double* const (&x)[K], double* const (&y)[K]) {
+        if (!hi) {
+#pragma unroll
+            for (int r = 0; r < K; ++r)
+                for (int i = threadIdx.x; i < n; i += blockDim.x) y[r][i] = x[r][i];
+            return;
+        }
+        if constexpr (!kMixed) {
+            count(C_DX, K);
+            matvec_dense_k<K>(D, ldd, x, y, n);
+        } else {
+#pragma unroll
+            for (int r = 0; r < K; ++r) {
+                if (r > 0) __syncthreads();
+                apply_D(x[r], y[r]);
+            }
+        }
+    }
+    // the same with the count of products known only at run time (1 + extra)
+    __device__ void apply_D_n(int k, const double* const* x, double* const* y) {
+        switch (k) {
+            case 1: { const double* const xs[1] = {x[0]}; double* const ys[1] = {y[0]}; apply_D_multi<1>(xs, ys); break; }
+            case 2: { const double* const xs[2] = {x[0], x[1]}; double* const ys[2] = {y[0], y[1]};
+                      apply_D_multi<2>(xs, ys); break; }
+            case 3: { const double* const xs[3] = {x[0], x[1], x[2]}; double* const ys[3] = {y[0], y[1], y[2]};
+                      apply_D_multi<3>(xs, ys); break; }
+            default: { const double* const xs[4] = {x[0], x[1], x[2], x[3]};
+                       double* const ys[4] = {y[0], y[1], y[2], y[3]}; apply_D_multi<4>(xs, ys); break; }
         }
     }
 
@@ -897,7 +971,10 @@ struct Block {
 
     // lanczos_extremes (src/hydrodynamics.cpp:146-221). Writes alpha/beta,
     // ctl.rmin/rmax, ctl.lz_steps, and the Ritz vectors into vmin/vmax.
-    __device__ void lanczos(int m, bool warm, const double* cache, double* w, double* vmin, double* vmax) {
+    // The first product D v0 is formed together with `nex` other products of
+    // the step (ex[r] -> ey[r]), against the same D.
+    __device__ void lanczos(int m, bool warm, const double* cache, double* w, double* vmin, double* vmax,
+                            int nex = 0, const double* const* ex = nullptr, double* const* ey = nullptr) {
         if (n < m) m = n;
         double* V0 = Vvec(0, m);
         if (warm) {
@@ -920,7 +997,13 @@ struct Block {
         for (int j = 0; j < m; ++j) {
             double* v = Vvec(j, m);
             const double* vprev = (j > 0) ? Vvec(j - 1, m) : nullptr;
-            apply_D(v, w);
+            if (j == 0 && nex > 0) {
+                const double* xs[4] = {v, ex[0], nex > 1 ? ex[1] : nullptr, nex > 2 ? ex[2] : nullptr};
+                double* ys[4] = {w, ey[0], nex > 1 ? ey[1] : nullptr, nex > 2 ? ey[2] : nullptr};
+                apply_D_n(1 + nex, xs, ys);
+            } else {
+                apply_D(v, w);
+            }
             __syncthreads();
             const double al = block_dot(v, w, n, red);
             if (threadIdx.x == 0) alpha[k] = al;
@@ -995,9 +1078,12 @@ struct Block {
 
     // spectral_bounds (src/hydrodynamics.cpp:224-264). Updates the chain's
     // warm-start vector in `cache` and ctl.lmin/lmax.
-    __device__ void spectral_bounds(double* cache, double* w, double* vmin, double* vmax, double* s) {
+    // The first Lanczos product is fused with `nex` (<= 3) further products
+    // of the step (ex[r] -> ey[r]).
+    __device__ void spectral_bounds(double* cache, double* w, double* vmin, double* vmax, double* s, int nex = 0,
+                                    const double* const* ex = nullptr, double* const* ey = nullptr) {
         const bool can_warm = ctl.cache_valid != 0;
-        lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, cache, w, vmin, vmax);
+        lanczos(can_warm ? kLanczosWarm : kLanczosCold, can_warm, cache, w, vmin, vmax, nex, ex, ey);
         if (can_warm && ctl.lz_steps < 4) {
             lanczos(kLanczosCold, false, cache, w, vmin, vmax);
             count(C_LZCOLD, 1);
@@ -1026,9 +1112,10 @@ struct Block {
     // ---- Chebyshev square root (src/hydrodynamics.cpp:267-337) ----------
     // out = D^{1/2} x0 approximation; returns with ctl.fd_err, ctl.L set.
     // Scratch: Dx0, t1, t2, t3, Dv.
+    // dx0_ready: Dx0 already holds D x0 (formed with the step's other products).
     __device__ void chebyshev(const double* x0, double* out, double* Dx0, double* t1, double* t2, double* t3,
-                              double* Dv) {
-        apply_D(x0, Dx0);
+                              double* Dv, bool dx0_ready = false) {
+        if (!dx0_ready) apply_D(x0, Dx0);
         __syncthreads();
         const double x0Dx0 = block_dot(x0, Dx0, n, red);
         const double lmin = ctl.lmin, lmax = ctl.lmax;
@@ -1216,6 +1303,8 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 __syncthreads();
                 if (ctl.stop) break;
             }
+            bool pre = false;        // J, K hold D (Fs + Fe) and D Fs from the bounds' first pass
+            bool chol_used = false;  // this step factored D into Lt
             // recenter (src/integrator.cpp:88-93)
             if (ch.update_com) {
                 if (tid < 3) {
@@ -1282,6 +1371,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             if (!B.hi) {
                 for (int i = tid; i < n; i += blockDim.x) dW[i] = sqrt_dt * X0[i];
             } else if (ch.hi_method == BDCU_HI_CHOLESKY) {
+                chol_used = true;
                 bool ok;
                 if constexpr (!kMixed) ok = B.cholesky(B.D, B.ldd, false);
                 else ok = B.cholesky(nullptr, 0, true);
@@ -1294,14 +1384,23 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 __syncthreads();
                 for (int i = tid; i < n; i += blockDim.x) dW[i] = sqrt_dt * A[i];
             } else {
-                B.spectral_bounds(gcache, A, Bv, Cv, E);
-                B.chebyshev(X0, F, A, Bv, Cv, E, G);
+                // the step's products that do not depend on one another go with
+                // the Lanczos start vector's: D x0 (Chebyshev) -> H, D (Fs + Fe)
+                // (predictor) -> J, D Fs (upsilon) -> K, with Fs + Fe in I
+                for (int i = tid; i < n; i += blockDim.x) I[i] = Fs[i] + Fe[i];
+                __syncthreads();
+                const double* ex[3] = {X0, I, Fs};
+                double* ey[3] = {H, J, K};
+                B.spectral_bounds(gcache, A, Bv, Cv, E, 3, ex, ey);
+                B.chebyshev(X0, F, H, Bv, Cv, E, G, true);
+                pre = true;
                 if (!(ctl.fd_err <= ch.fd_tol)) {
                     // Cholesky fallback (src/mobility.cpp:69-81)
                     if (tid == 0) {
                         ctl.status |= BDCU_ST_CHEB_FALLBACK;
                         ctl.cnt[C_FALLBACK] += 1;
                     }
+                    chol_used = true;
                     bool ok;
                     if constexpr (!kMixed) {
                         ok = B.cholesky(B.D, B.ldd, false);
@@ -1316,6 +1415,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                     }
                     B.lower_matvec(X0, F);
                     __syncthreads();
+                    pre = false;  // the blocked factorisation stages tiles in slots I..K
                 }
                 for (int i = tid; i < n; i += blockDim.x) dW[i] = sqrt_dt * F[i];
             }
@@ -1324,14 +1424,19 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             double K1[9], K2[9];
             kappa_at(ch, a.arena, t, K1);
             kappa_at(ch, a.arena, t + dt, K2);
-            for (int i = tid; i < n; i += blockDim.x) A[i] = Fs[i] + Fe[i];
-            __syncthreads();
-            B.apply_D(A, Bv);
+            if (!pre) {
+                // D (Fs + Fe) -> J for the predictor and D Fs -> K for upsilon, in one pass
+                for (int i = tid; i < n; i += blockDim.x) I[i] = Fs[i] + Fe[i];
+                __syncthreads();
+                const double* xs[2] = {I, Fs};
+                double* ys[2] = {J, K};
+                B.apply_D_multi<2>(xs, ys);
+            }
             __syncthreads();
             for (int i = tid; i < n; i += blockDim.x) {
                 const int r = i % 3, b3 = i - r;
                 const double fl1 = K1[3 * r] * R[b3] + K1[3 * r + 1] * R[b3 + 1] + K1[3 * r + 2] * R[b3 + 2];
-                Rp[i] = R[i] + dt * (fl1 + 0.25 * Bv[i]) + sqrt2inv * dW[i];
+                Rp[i] = R[i] + dt * (fl1 + 0.25 * J[i]) + sqrt2inv * dW[i];
             }
             __syncthreads();
             if constexpr (kMixed) {
@@ -1350,20 +1455,9 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                     B.pos32[b] = make_float4((float)R[3 * b], (float)R[3 * b + 1], (float)R[3 * b + 2], 0.f);
                 __syncthreads();
             }
-            B.apply_D(Fs, A);
-            for (int i = tid; i < n; i += blockDim.x) E[i] = Fe[i] + Cv[i];
-            __syncthreads();
-            B.apply_D(E, F);
-            __syncthreads();
-            for (int i = tid; i < n; i += blockDim.x) {
-                const int r = i % 3, b3 = i - r;
-                const double fl1 = K1[3 * r] * R[b3] + K1[3 * r + 1] * R[b3 + 1] + K1[3 * r + 2] * R[b3 + 2];
-                const double fl2 = K2[3 * r] * Rp[b3] + K2[3 * r + 1] * Rp[b3 + 1] + K2[3 * r + 2] * Rp[b3 + 2];
-                const double flow = 0.5 * (fl1 + fl2);
-                Bv[i] = R[i] + dt * (flow + 0.125 * A[i] + 0.125 * F[i]) + sqrt2inv * dW[i];
-            }
-            __syncthreads();
-            // solve_connectors (src/integrator.cpp:125-165)
+            // solve_connectors (src/integrator.cpp:125-165): its first
+            // iteration's bonds are those of R~, so its first product D Fb is
+            // formed here together with upsilon's D (Fe + Fe~)
             double* ups = Bv;
             double* dups = Cv;
             double* bond = E;
@@ -1374,31 +1468,57 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             double* Rc = K;
             double* d2 = F;
             for (int b = tid; b < N - 1; b += blockDim.x)
-                for (int d = 0; d < 3; ++d) {
-                    dups[3 * b + d] = ups[3 * (b + 1) + d] - ups[3 * b + d];
-                    bond[3 * b + d] = Rp[3 * (b + 1) + d] - Rp[3 * b + d];
-                }
+                for (int d = 0; d < 3; ++d) bond[3 * b + d] = Rp[3 * (b + 1) + d] - Rp[3 * b + d];
+            __syncthreads();
+            for (int b = tid; b < N - 1; b += blockDim.x) {
+                const double l = clamped_len(bond[3 * b], bond[3 * b + 1], bond[3 * b + 2]);
+                const double f = connector_factor(ch, l);
+                Fc[3 * b] = f * bond[3 * b];
+                Fc[3 * b + 1] = f * bond[3 * b + 1];
+                Fc[3 * b + 2] = f * bond[3 * b + 2];
+            }
+            __syncthreads();
+            B.bead_forces(Fc, Fb);
+            for (int i = tid; i < n; i += blockDim.x) G[i] = Fe[i] + Cv[i];
+            __syncthreads();
+            {
+                const double* xs[2] = {G, Fb};
+                double* ys[2] = {F, DFs};
+                B.apply_D_multi<2>(xs, ys);
+            }
+            __syncthreads();
+            for (int i = tid; i < n; i += blockDim.x) {
+                const int r = i % 3, b3 = i - r;
+                const double fl1 = K1[3 * r] * R[b3] + K1[3 * r + 1] * R[b3 + 1] + K1[3 * r + 2] * R[b3 + 2];
+                const double fl2 = K2[3 * r] * Rp[b3] + K2[3 * r + 1] * Rp[b3 + 1] + K2[3 * r + 2] * Rp[b3 + 2];
+                const double flow = 0.5 * (fl1 + fl2);
+                Bv[i] = R[i] + dt * (flow + 0.125 * K[i] + 0.125 * F[i]) + sqrt2inv * dW[i];
+            }
+            __syncthreads();
+            for (int b = tid; b < N - 1; b += blockDim.x)
+                for (int d = 0; d < 3; ++d) dups[3 * b + d] = ups[3 * (b + 1) + d] - ups[3 * b + d];
             for (int i = tid; i < n; i += blockDim.x) Rprev[i] = Rp[i];
             __syncthreads();
             const int max_iter = 100 * N;
             int lstat = 0;
             for (int iter = 0;; ++iter) {
-                for (int b = tid; b < N - 1; b += blockDim.x) {
-                    const double l = clamped_len(bond[3 * b], bond[3 * b + 1], bond[3 * b + 2]);
-                    const double f = connector_factor(ch, l);
-                    Fc[3 * b] = f * bond[3 * b];
-                    Fc[3 * b + 1] = f * bond[3 * b + 1];
-                    Fc[3 * b + 2] = f * bond[3 * b + 2];
-                }
-                __syncthreads();
-                B.bead_forces(Fc, Fb);
-                __syncthreads();
-                const double* DF = Fb;
-                if (B.hi) {
-                    B.apply_D(Fb, DFs);
-                    DF = DFs;
+                if (iter > 0) {  // (the first iteration's Fc, Fb and D Fb are formed above)
+                    for (int b = tid; b < N - 1; b += blockDim.x) {
+                        const double l = clamped_len(bond[3 * b], bond[3 * b + 1], bond[3 * b + 2]);
+                        const double f = connector_factor(ch, l);
+                        Fc[3 * b] = f * bond[3 * b];
+                        Fc[3 * b + 1] = f * bond[3 * b + 1];
+                        Fc[3 * b + 2] = f * bond[3 * b + 2];
+                    }
                     __syncthreads();
+                    B.bead_forces(Fc, Fb);
+                    __syncthreads();
+                    if (B.hi) {
+                        B.apply_D(Fb, DFs);
+                        __syncthreads();
+                    }
                 }
+                const double* DF = B.hi ? DFs : Fb;
                 const double c8 = 0.125 * dt, c4 = 0.25 * dt;
                 for (int b = tid; b < N - 1; b += blockDim.x) {
                     double g[3], q[3];
@@ -1461,6 +1581,13 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             if (tid == 0) ctl.cnt[C_STEPS] += 1;
             t += dt;
             __syncthreads();
+            if constexpr (!kMixed) {
+                // D (and a factor made this step) are dead until the next
+                // step rebuilds them: drop their L2 lines unwritten
+                if (B.hi && !a.d_in_smem) discard_l2(B.D, (int64_t)n * B.ldd);
+                if (chol_used) discard_l2(B.Lt, (int64_t)n * n);
+                __syncthreads();
+            }
         }
         __syncthreads();
         // write back: positions (unless the chain failed), RNG, cache flag, status, counters

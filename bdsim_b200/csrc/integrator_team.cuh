@@ -1373,46 +1373,25 @@ __global__ void __launch_bounds__(TeamCfg<T, Q>::kCtaThreads, TeamCfg<T, Q>::kMi
             // D Fs + D (Fe + Fe~) = D (Fs + Fe) + D Fe~: the predictor's
             // product plus one more (the reference forms both sums anew)
             W.stage_pos(R);
-            float DFep[Q][3];
-            double ups[Q][3];
-            W.applyF(Fep, DFep);
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
-                    const double fl2 = K2[3 * r] * Rp[q][0] + K2[3 * r + 1] * Rp[q][1] + K2[3 * r + 2] * Rp[q][2];
-                    ups[q][r] = R[q][r] + dt * (0.5 * (fl1 + fl2) + 0.125 * ((double)DF[q][r] + (double)DFep[q][r])) +
-                                sqrt2inv * dW[q][r];
-                }
-            // solve_connectors (src/integrator.cpp:125-165): thread owns bonds bead(0), bead(1)
-            W.to_smem(S.s0, ups);
+            // solve_connectors (src/integrator.cpp:125-165): thread owns bonds
+            // bead(0), bead(1). Its first iteration's bonds are those of R~,
+            // so that iteration's product D Fb is formed in one pass with
+            // upsilon's D Fe~.
             W.to_smem(S.s1, Rp);
             team_sync<T>(team);
-            double dups[Q][3], bond[Q][3];
+            double bond[Q][3];
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const int b = W.bead(q);
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const bool ok = b < N - 1;
-                    dups[q][d] = ok ? S.s0[3 * (b + 1) + d] - S.s0[3 * b + d] : 0.0;
-                    bond[q][d] = ok ? S.s1[3 * (b + 1) + d] - S.s1[3 * b + d] : 0.0;
-                }
+                for (int d = 0; d < 3; ++d) bond[q][d] = b < N - 1 ? S.s1[3 * (b + 1) + d] - S.s1[3 * b + d] : 0.0;
             }
             const double anchor0 = S.s1[0], anchor1 = S.s1[1], anchor2 = S.s1[2];
             team_sync<T>(team);
-            double Rprev[Q][3], Rc[Q][3];
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) Rprev[q][d] = Rp[q][d];
-            const int max_iter = 100 * N;
-            const double c8 = 0.125 * dt, c4 = 0.25 * dt;
-            int lstat = 0;
-            for (int iter = 0;; ++iter) {
-                // connector forces (src/spring.cpp:183-193) into s1, bead forces
-                double Fc[Q][3];
+            double Fc[Q][3];
+            float Fb[Q][3], DFb[Q][3];
+            // connector forces (src/spring.cpp:183-193) into s1, then the bead forces
+            auto connector_and_bead_forces = [&]() {
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
                     const int b = W.bead(q);
@@ -1425,7 +1404,6 @@ __global__ void __launch_bounds__(TeamCfg<T, Q>::kCtaThreads, TeamCfg<T, Q>::kMi
                     }
                 }
                 team_sync<T>(team);
-                float Fb[Q][3], DFb[Q][3];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
                     const int m = W.bead(q);
@@ -1441,7 +1419,68 @@ __global__ void __launch_bounds__(TeamCfg<T, Q>::kCtaThreads, TeamCfg<T, Q>::kMi
                     }
                 }
                 team_sync<T>(team);
-                W.applyF(Fb, DFb);
+            };
+            connector_and_bead_forces();
+            float DFep[Q][3];
+            if (W.hi) {
+                float x2[2][Q][3], y2[2][Q][3];
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        x2[0][q][d] = Fep[q][d];
+                        x2[1][q][d] = Fb[q][d];
+                    }
+                W.template applyK<2>(x2, y2);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        DFep[q][d] = y2[0][q][d];
+                        DFb[q][d] = y2[1][q][d];
+                    }
+            } else {
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        DFep[q][d] = Fep[q][d];
+                        DFb[q][d] = Fb[q][d];
+                    }
+            }
+            double ups[Q][3];
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const double fl1 = K1[3 * r] * R[q][0] + K1[3 * r + 1] * R[q][1] + K1[3 * r + 2] * R[q][2];
+                    const double fl2 = K2[3 * r] * Rp[q][0] + K2[3 * r + 1] * Rp[q][1] + K2[3 * r + 2] * Rp[q][2];
+                    ups[q][r] = R[q][r] + dt * (0.5 * (fl1 + fl2) + 0.125 * ((double)DF[q][r] + (double)DFep[q][r])) +
+                                sqrt2inv * dW[q][r];
+                }
+            W.to_smem(S.s0, ups);
+            team_sync<T>(team);
+            double dups[Q][3];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int b = W.bead(q);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) dups[q][d] = b < N - 1 ? S.s0[3 * (b + 1) + d] - S.s0[3 * b + d] : 0.0;
+            }
+            team_sync<T>(team);
+            double Rprev[Q][3], Rc[Q][3];
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) Rprev[q][d] = Rp[q][d];
+            const int max_iter = 100 * N;
+            const double c8 = 0.125 * dt, c4 = 0.25 * dt;
+            int lstat = 0;
+            for (int iter = 0;; ++iter) {
+                if (iter > 0) {  // (the first iteration's Fc, Fb and D Fb are formed above)
+                    connector_and_bead_forces();
+                    W.applyF(Fb, DFb);
+                }
 #pragma unroll
                 for (int q = 0; q < Q; ++q)
                     if (W.valid(q))
