@@ -284,9 +284,10 @@ def load_library():
     lib.bdcu_write_arena.argtypes = [vp, ctypes.c_int64, c_double_p, ctypes.c_int64]
     lib.bdcu_select.argtypes = [vp, ctypes.c_int, c_int32_p]
     lib.bdcu_set_team_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.bdcu_set_single_launch.argtypes = [vp, ctypes.c_int]
     lib.bdcu_check_chains.argtypes = [ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim), c_double_p,
                                       ctypes.c_int64, ctypes.c_char_p, ctypes.c_int]
-    for name in ("bdcu_set_team_shape", "bdcu_check_chains", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
+    for name in ("bdcu_set_single_launch", "bdcu_set_team_shape", "bdcu_check_chains", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
                  "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
                  "bdcu_forces", "bdcu_ran1", "bdcu_run_static", "bdcu_describe_plan", "bdcu_autotune",
                  "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select"):
@@ -301,7 +302,7 @@ EXPORTED_SYMBOLS = [
     "bdcu_set_chains", "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host",
     "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_describe_plan", "bdcu_autotune",
     "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select", "bdcu_run_static",
-    "bdcu_check_chains", "bdcu_set_team_shape",
+    "bdcu_check_chains", "bdcu_set_team_shape", "bdcu_set_single_launch",
 ]
 
 

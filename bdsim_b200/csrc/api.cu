@@ -392,6 +392,17 @@ int build_plan(bdcu_ctx* ctx, int form) {
     } else {
         for (int32_t c : ctx->sel) lists[bucket_of(ctx->chains_h[c], form)].push_back(c);
     }
+    if (ctx->single_launch) {
+        // one persistent launch for every team-kernel chain: the widest team
+        // bucket present takes the others' chains (and runs its shape)
+        int top = -1;
+        for (int id = 0; id < kFirstBlockBucket; ++id)
+            if (!lists[id].empty()) top = id;
+        for (int id = 0; id < top; ++id) {
+            lists[top].insert(lists[top].end(), lists[id].begin(), lists[id].end());
+            lists[id].clear();
+        }
+    }
     ctx->plan.clear();
     ctx->order_h.clear();
     int rc;
@@ -862,6 +873,13 @@ int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, 
     }
 #undef TK
     cleanup();
+    ctx->plan_dirty = 1;
+    return BDCU_OK;
+}
+
+int bdcu_set_single_launch(bdcu_ctx* ctx, int on) {
+    if (!ctx) return BDCU_E_ARG;
+    ctx->single_launch = on ? 1 : 0;
     ctx->plan_dirty = 1;
     return BDCU_OK;
 }

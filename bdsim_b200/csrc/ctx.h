@@ -87,6 +87,7 @@ struct bdcu_ctx {
     int32_t* work_d = nullptr;  // one queue counter per bucket
     int sm_count = 148;
     int bounds_every = 1;  // bdcu_set_bounds_refresh
+    int single_launch = 0; // bdcu_set_single_launch: every team-kernel chain in one launch
     size_t max_smem = 0;
     // the chains bdcu_run advances: all records (sel_all) or a list (bdcu_select)
     int sel_all = 1;

@@ -150,6 +150,11 @@ class Context:
         self._ck(self.lib.bdcu_set_team_shape(self.h, int(bucket), int(team_warps), int(beads_per_thread)),
                  "bdcu_set_team_shape")
 
+    def set_single_launch(self, on: bool = True):
+        """All team-kernel chains in one persistent launch (the widest team
+        bucket's shape) instead of one launch per bucket."""
+        self._ck(self.lib.bdcu_set_single_launch(self.h, int(bool(on))), "bdcu_set_single_launch")
+
     # ---- slot pools (serving)
 
     def reserve(self, n_slots: int, bead_capacity: int, arena_len: int = 0):
@@ -286,6 +291,13 @@ class Ensemble:
     def positions(self):
         R = self.R.cpu().numpy()
         return [R[self.offsets[i]:self.offsets[i + 1]].copy() for i in range(self.n)]
+
+    def total_force_device(self):
+        """Total force per bead of every chain, a device tensor (total_beads, 3)
+        (asynchronous on the current stream)."""
+        F = self.torch.empty_like(self.R)
+        self.ctx.total_force(self.R, F)
+        return F
 
     def total_force(self):
         F = self.torch.empty_like(self.R)

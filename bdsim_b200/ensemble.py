@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import os
 import sys
+import threading
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -140,38 +141,48 @@ def simulate(phys: PhysParams, sim: SimParams, *, n_traj: int = 1, seed: int = 0
     n_steps = int(n_steps) if n_steps is not None else n_steps_of(sim)
     os.makedirs(output.directory, exist_ok=True)
     ens, R0s = _start(phys, sim, n_traj, seed, initial, form, device)
+    torch = ens.torch
     w = output.write_every if (output.write_every and output.write_every > 0) else n_steps
-    snaps_R, snaps_F, steps, times = [np.stack(R0s)], [], [0], [sim.time_start]
-    if output.write_forces:
-        snaps_F.append(np.stack(ens.total_force()))
-    step = 0
+    n_snap = 1 + (n_steps + w - 1) // w
+    # each snapshot: device -> pinned host copy on the launch stream (after the
+    # chunk's kernel, before the next), then spooled to disk by the writer's
+    # thread while the device runs the next chunk; two pinned buffers rotate
+    writer = storage.RunWriter(output.directory, ens.offsets, n_snap, bool(output.write_forces))
+    total = int(ens.offsets[-1])
+    pin_R = [torch.empty((total, 3), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    pin_F = [torch.empty((total, 3), dtype=torch.float64, pin_memory=True) for _ in range(2)] \
+        if output.write_forces else None
+    free = [threading.Semaphore(1) for _ in range(2)]
+
+    def snapshot(k, step, time_):
+        slot = k % 2
+        free[slot].acquire()
+        pin_R[slot].copy_(ens.R, non_blocking=True)
+        if pin_F is not None:
+            pin_F[slot].copy_(ens.total_force_device(), non_blocking=True)
+        ready = torch.cuda.Event()
+        ready.record()
+        writer.put(k, step, time_, pin_R[slot].numpy(), None if pin_F is None else pin_F[slot].numpy(),
+                   ready=ready, release=free[slot].release)
+
+    snapshot(0, 0, sim.time_start)
+    step, k = 0, 0
     while step < n_steps:
         chunk = min(w, n_steps - step)
         t0 = sim.time_start + step * sim.dt
-        k = count_steps(_segment(sim, t0, t0 + (chunk - 1) * sim.dt))
-        ens.advance(t0, k, CACHE_RESET_PER_CALL)
+        ens.advance(t0, count_steps(_segment(sim, t0, t0 + (chunk - 1) * sim.dt)), CACHE_RESET_PER_CALL)
         step += chunk
-        steps.append(step)
-        times.append(sim.time_start + step * sim.dt)
-        snaps_R.append(np.stack(ens.positions()))
-        if output.write_forces:
-            snaps_F.append(np.stack(ens.total_force()))
+        k += 1
+        snapshot(k, step, sim.time_start + step * sim.dt)
     status = ens.statuses()
-    sink = storage.SnapshotSink()
-    results = []
-    P = np.stack(snaps_R, axis=1)  # (n_traj, n_snap, N, 3)
-    Fa = np.stack(snaps_F, axis=1) if output.write_forces else None
-    for i in range(n_traj):
-        if status[i] & ST_FATAL_MASK:
-            results.append(Failure(i, IntegratorError(int(status[i]), i)))
-            continue
-        attrs = {"index": i, "seed": seed + i, "n_steps": n_steps, "write_every": output.write_every or n_steps,
-                 "dt": float(sim.dt), **{f"phys_{k}": v for k, v in _phys_summary(phys).items()}}
-        path = storage.trajectory_path(output.directory, i)
-        sink.put(path, steps=steps, times=times, positions=P[i], forces=None if Fa is None else Fa[i],
-                 attrs=attrs, compression=output.compression)
-        results.append(os.path.basename(path))
-    sink.close()
+    keep = [not (status[i] & ST_FATAL_MASK) for i in range(n_traj)]
+
+    def attrs(i):
+        return {"index": i, "seed": seed + i, "n_steps": n_steps, "write_every": output.write_every or n_steps,
+                "dt": float(sim.dt), **{f"phys_{k}": v for k, v in _phys_summary(phys).items()}}
+
+    written = iter(writer.finish(keep, attrs, compression=output.compression))
+    results = [next(written) if keep[i] else Failure(i, IntegratorError(int(status[i]), i)) for i in range(n_traj)]
     if on_error == "raise":
         bad = [r for r in results if isinstance(r, Failure)]
         if bad:

@@ -37,6 +37,7 @@ carries across chunks.
 from __future__ import annotations
 
 import bisect
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -44,7 +45,8 @@ import numpy as np
 
 from ._abi import CACHE_PERSIST, CACHE_RESET_PER_CALL, COUNTER_FIELDS, ST_FATAL_MASK, count_steps
 from .engine import Context, _torch, form_code
-from .ensemble import INITIALIZERS, Initial, _segment, n_steps_of
+from . import storage
+from .ensemble import INITIALIZERS, Initial, Output, _phys_summary, _segment, n_steps_of
 from .params import PhysParams, Rng, SimParams
 
 BYTES_PER_BEAD = 4 * 24  # R, warm-start cache, two snapshot buffers (FP64 xyz each)
@@ -104,6 +106,11 @@ class Job:
     write_every: int = 0
     keep_snapshots: bool = True
     name: str = ""
+    # the run directory of `simulate` (python/bdsim/storage.py layout): each
+    # chunk's positions are spooled to disk by a writer thread as they arrive,
+    # and traj_NNNNN + manifest.json are written when the job completes
+    # (positions only: write_forces is not served)
+    output: Output = None
 
 
 @dataclass
@@ -127,6 +134,9 @@ class JobState:
     positions: list = field(default_factory=list)  # per snapshot: (n_traj, N, 3)
     status: np.ndarray = None
     counters: dict = None
+    writer: object = None  # storage.RunWriter of a job with an output directory
+    files: list = None     # the trajectory files it wrote
+    write_error: object = None
 
     @property
     def latency(self):
@@ -207,6 +217,7 @@ class Server:
         self.n_slices = 0
         self.selected_chains = 0
         self.retired_counters = np.zeros(len(COUNTER_FIELDS), dtype=np.int64)
+        self.finalizing = []  # threads writing finished jobs' run directories
 
     # ------------------------------------------------------------------ API
 
@@ -244,6 +255,16 @@ class Server:
         while self.busy() and it < max_iters:
             self.step()
             it += 1
+        self.flush()
+
+    def flush(self):
+        """Wait until the run directories of finished jobs are written (their
+        errors are raised here)."""
+        while self.finalizing:
+            self.finalizing.pop(0).join()
+        errs = [js.write_error for js in self.done if getattr(js, "write_error", None) is not None]
+        if errs:
+            raise errs[0]
 
     def run_stream(self, jobs, arrivals, horizon: float = None, drain: bool = True, drain_limit: float = None):
         """Replay an arrival stream in real time: jobs[i] arrives arrivals[i]
@@ -269,6 +290,7 @@ class Server:
                                                          (drain_limit is not None and now > horizon + drain_limit)):
                 break
             self.step()
+        self.flush()
         return self.stats(t0)
 
     def stats(self, t0: float = None) -> dict:
@@ -357,6 +379,13 @@ class Server:
             js.state, js.t_admit = "running", self.clock()
             js.steps.append(0)
             js.times.append(float(job.sim.time_start))
+            if job.output is not None:
+                if job.output.directory is None or job.output.write_forces:
+                    raise ValueError("a served job's output needs a directory and no forces")
+                w = job.write_every if (job.write_every and job.write_every > 0) else js.n_steps
+                js.writer = storage.RunWriter(job.output.directory, np.arange(n + 1) * N,
+                                              1 + (js.n_steps + w - 1) // w, max_pending=4)
+                js.writer.put(0, 0, float(job.sim.time_start), R0.copy())
             if job.keep_snapshots:
                 js.positions.append(R0.reshape(n, N, 3).copy())
             if self.on_snapshot is not None:
@@ -417,6 +446,7 @@ class Server:
         return work, sel, ev
 
     def _finish_slice(self, work, sel, ev=None):
+        torch = self.torch
         if ev is not None:
             ev.synchronize()
             e0, e1 = self._slice_events
@@ -439,7 +469,17 @@ class Server:
             js.step = js.chunk_end
             js.chunk_end = -1
             N = js.n_beads
-            rows = self.R[js.bead0:js.bead0 + n * N].cpu().numpy().reshape(n, N, 3)
+            if js.writer is not None:
+                # device -> pinned host copy on the stream; the writer thread
+                # waits for it and spools the chunk while the server goes on
+                pinned = torch.empty((n * N, 3), dtype=torch.float64, pin_memory=True)
+                pinned.copy_(self.R[js.bead0:js.bead0 + n * N], non_blocking=True)
+                ready = torch.cuda.Event()
+                ready.record()
+                js.writer.put(len(js.steps), js.step, js.t_chunk_end, pinned.numpy(), ready=ready)
+            rows = None
+            if js.job.keep_snapshots or self.on_snapshot is not None:
+                rows = self.R[js.bead0:js.bead0 + n * N].cpu().numpy().reshape(n, N, 3)
             js.steps.append(js.step)
             js.times.append(js.t_chunk_end)
             if js.job.keep_snapshots:
@@ -449,8 +489,38 @@ class Server:
             st = self.status_host.numpy()[js.slot0:js.slot0 + n]
             if js.step >= js.n_steps or bool(((st & ST_FATAL_MASK) != 0).all()):
                 js.status = st.copy()
+                if js.writer is not None:  # the run directory is assembled off the serving loop
+                    th = threading.Thread(target=self._write_run, args=(js,), daemon=True)
+                    th.start()
+                    self.finalizing.append(th)
                 js.state, js.t_done = "done", now
                 self._retire(js)
+
+    def _write_run(self, js: JobState):
+        """The job's run directory, as `simulate` writes it (its chunks are on
+        the spool already)."""
+        job = js.job
+        keep = (js.status & ST_FATAL_MASK) == 0
+        w = job.write_every if (job.write_every and job.write_every > 0) else js.n_steps
+
+        def attrs(i):
+            return {"index": i, "seed": job.seed + i, "n_steps": js.n_steps, "write_every": w,
+                    "dt": float(job.sim.dt), **{f"phys_{k}": v for k, v in _phys_summary(job.phys).items()}}
+
+        # (every chain failed before the end: the snapshots that ran)
+        try:
+            js.files = js.writer.finish(keep, attrs, compression=job.output.compression, n_used=len(js.steps))
+        except Exception as exc:  # raised by flush()
+            js.write_error = exc
+            return
+        init = job.initial or Initial()
+        storage.write_manifest(job.output.directory, {
+            "n_trajectories": len(js.files), "n_trajectories_requested": int(job.n_traj),
+            "n_trajectories_failed": int((~keep).sum()), "seed": job.seed, "n_steps": js.n_steps,
+            "dt": float(job.sim.dt), "write_every": w, "write_forces": False,
+            "initial": {"method": init.method, "kwargs": init.kwargs}, "phys": _phys_summary(job.phys),
+            "files": list(js.files), "backend": "cuda (served)"})
+        js.writer = None
 
     def _retire(self, js: JobState):
         n = int(js.job.n_traj)

@@ -8,8 +8,13 @@ Each trajectory file holds `step` (n_snap,), `time` (n_snap,), `positions`
 container is HDF5 (.h5, gzip) when h5py is importable, otherwise a NumPy .npz
 archive with the same dataset names (h5py is not part of every image).
 
-`SnapshotSink` writes trajectories on a background thread, so device work of
-the next chunk overlaps the file writes of the previous one.
+`RunWriter` takes a run's snapshots chunk by chunk as they come off the GPU
+(copied into pinned host buffers on the launch stream, each followed by an
+event) and spools them to disk on a background thread while the device runs
+the next chunk; at the end it writes one file per trajectory from the spool.
+Host memory holds at most `max_pending` snapshots, not the whole run.
+`SnapshotSink` writes whole trajectories on a background thread.
+h5py is not installed in every image (not in this one): the fallback is .npz.
 """
 from __future__ import annotations
 
@@ -194,3 +199,96 @@ class SnapshotSink:
         self.t.join()
         if self.err is not None:
             raise self.err
+
+
+class RunWriter:
+    """Chunk-by-chunk snapshot writer for a run of n_traj trajectories with
+    bead offsets `offsets` (n_traj + 1) into the concatenated positions.
+
+    put(k, step, time, positions, forces=None, ready=None): snapshot k of the
+    run; positions (and forces) are host arrays (total_beads, 3), typically
+    pinned tensors filled by a non-blocking device copy, and `ready` an event
+    (anything with .synchronize()) recorded after that copy. The writer thread
+    waits for the event, then stores the snapshot in the spool file
+    (directory/.spool_*.f64, one (n_snap, total_beads, 3) float64 array).
+    `release` (if given to put) is called once the buffers may be reused.
+
+    finish(keep, attrs, compression) waits for the queue, writes
+    traj_NNNNN.<ext> for every trajectory i with keep[i] (attrs(i) its
+    attributes), removes the spool and returns the file names. Errors of the
+    thread are raised by finish.
+    """
+
+    def __init__(self, directory, offsets, n_snap: int, write_forces: bool = False, max_pending: int = 2):
+        self.directory = directory
+        os.makedirs(directory, exist_ok=True)
+        self.offsets = np.asarray(offsets, dtype=np.int64)
+        self.n_snap = int(n_snap)
+        total = int(self.offsets[-1])
+        self.paths = [os.path.join(directory, ".spool_positions.f64")]
+        self.pos = np.lib.format.open_memmap(self.paths[0] + ".npy", mode="w+", dtype=np.float64,
+                                             shape=(self.n_snap, total, 3))
+        self.paths[0] += ".npy"
+        self.frc = None
+        if write_forces:
+            p = os.path.join(directory, ".spool_forces.f64.npy")
+            self.paths.append(p)
+            self.frc = np.lib.format.open_memmap(p, mode="w+", dtype=np.float64, shape=(self.n_snap, total, 3))
+        self.steps = np.zeros(self.n_snap, dtype=np.int64)
+        self.times = np.zeros(self.n_snap, dtype=np.float64)
+        self.filled = np.zeros(self.n_snap, dtype=bool)
+        self.q = queue.Queue(maxsize=max(1, int(max_pending)))
+        self.err = None
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _run(self):
+        while True:
+            item = self.q.get()
+            if item is None:
+                return
+            k, step, time_, pos, frc, ready, release = item
+            try:
+                if ready is not None:
+                    ready.synchronize()
+                self.pos[k] = np.asarray(pos)
+                if self.frc is not None and frc is not None:
+                    self.frc[k] = np.asarray(frc)
+                self.steps[k] = step
+                self.times[k] = time_
+                self.filled[k] = True
+            except Exception as exc:  # surfaced by finish()
+                if self.err is None:
+                    self.err = exc
+            finally:
+                if release is not None:
+                    release()
+
+    def put(self, k, step, time_, positions, forces=None, ready=None, release=None):
+        if not 0 <= k < self.n_snap:
+            raise IndexError(f"snapshot {k} outside the run's {self.n_snap}")
+        self.q.put((int(k), int(step), float(time_), positions, forces, ready, release))
+
+    def finish(self, keep, attrs, compression="gzip", n_used=None):
+        """n_used: write only the first n_used snapshots (a run cut short)."""
+        self.q.put(None)
+        self.t.join()
+        if self.err is not None:
+            raise self.err
+        m = self.n_snap if n_used is None else int(n_used)
+        if not self.filled[:m].all():
+            raise RuntimeError("RunWriter: snapshots missing at finish")
+        files = []
+        for i in range(len(self.offsets) - 1):
+            if not keep[i]:
+                continue
+            lo, hi = self.offsets[i], self.offsets[i + 1]
+            path = trajectory_path(self.directory, i)
+            write_trajectory(path, self.steps[:m], self.times[:m], self.pos[:m, lo:hi, :],
+                             None if self.frc is None else self.frc[:m, lo:hi, :], attrs=attrs(i),
+                             compression=compression)
+            files.append(os.path.basename(path))
+        del self.pos, self.frc
+        for p in self.paths:
+            os.unlink(p)
+        return files

@@ -255,9 +255,11 @@ def run_serving(torch, horizon, scale_steps=1.0, rate=200.0, seed=0, form="mixed
         jobs.append(serving.Job(phys=sp.phys, sim=sp.sim, n_traj=sp.n_traj, seed=sp.seed, n_steps=ns,
                                 write_every=sp.write_every, keep_snapshots=False))
         arrivals.append(sp.arrival)
+    # every completed chunk's positions are copied to the host (delivered) and dropped
     srv = serving.Server(device=torch.cuda.current_device(), form=form, max_chains=max_active,
                          hbm_budget_bytes=2 << 30, queue_limit=queue_limit, max_active_chains=max_active,
-                         policy=policy, slice_steps=slice_steps, slice_budget_s=slice_budget_s)
+                         policy=policy, slice_steps=slice_steps, slice_budget_s=slice_budget_s,
+                         on_snapshot=lambda js, step, t, rows: None)
     torch.cuda.synchronize()
     st = srv.run_stream(jobs, np.asarray(arrivals), horizon=horizon, drain=drain, drain_limit=drain_limit)
     torch.cuda.synchronize()

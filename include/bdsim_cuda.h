@@ -312,6 +312,15 @@ int bdcu_describe_plan(bdcu_ctx* ctx, int form, bdcu_bucket_info* out, int cap, 
 int bdcu_autotune(bdcu_ctx* ctx, int form, const double* R, const int32_t* rng, const double* cache,
                   const int32_t* cache_valid, const double* t_start, int probe_steps);
 
+/* on = 1: every chain of the FP32-mixed form's team kernel runs in ONE
+   persistent launch (the widest team bucket present takes the narrower
+   buckets' chains, largest first, and runs its shape) instead of one launch
+   per bucket forked onto streams; on = 0 restores the per-bucket plan. A
+   chain's result depends on the team shape it runs with (the order of its
+   team reductions), not on which launch it is in. No counterpart in the
+   reference. */
+int bdcu_set_single_launch(bdcu_ctx* ctx, int on);
+
 /* Pin the team shape of team-kernel bucket `bucket` (0..3) of the FP32-mixed
    form: team_warps warps per chain with beads_per_thread (1 or 2) beads per
    thread, a compiled shape that holds every chain the bucket admits (32 *

@@ -254,3 +254,20 @@ def test_team_shape_rejects_a_shape_that_does_not_hold_the_bucket(uneven):
     ens.ctx.set_team_shape(2, 8, 1)
     ens.ctx.set_team_shape(2, 0, 0)  # back to the default
     assert {x["bucket"]: x for x in ens.plan()}[2]["team_warps"] == 4
+
+
+def test_single_launch_runs_every_team_chain_in_one_bucket(uneven, port_results):
+    ens = _ensemble(uneven, "mixed")
+    ens.ctx.set_single_launch(True)
+    plan = ens.plan()
+    team = [b for b in plan if b["kernel"] == _abi.KERNEL_TEAM]
+    assert len(team) == 1 and team[0]["n_chains"] == sum(n <= 512 for n in NS)
+    assert team[0]["min_beads"] == min(NS) and team[0]["max_beads"] == max(n for n in NS if n <= 512)
+    ens.advance(0.0, STEPS, _abi.CACHE_RESET_PER_CALL)
+    got = ens.positions()
+    states = ens.rng_states()
+    for i, (R, st, _) in enumerate(port_results):
+        assert states[i] == st, i
+        assert rel(got[i], R) <= MIXED_TOL, (NS[i], rel(got[i], R))
+    ens.ctx.set_single_launch(False)
+    assert len([b for b in ens.plan() if b["kernel"] == _abi.KERNEL_TEAM]) == 4

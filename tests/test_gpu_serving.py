@@ -69,6 +69,19 @@ def test_served_job_equals_simulate(tmp_path):
     for i, tr in enumerate(run):
         assert list(tr.step) == js.steps
         assert np.array_equal(tr.positions, got[i])
+    # the same job with an output directory: the server spools each chunk as
+    # it completes and writes simulate's run directory
+    srv = _server("plain")
+    job = _job(*spec)
+    job.output = Output(directory=str(tmp_path / "served"), write_every=100)
+    job.keep_snapshots = False
+    js2 = srv.submit(job)
+    srv.run_until_idle()
+    served = B.read_run(str(tmp_path / "served"))
+    assert served.manifest["files"] == run.manifest["files"] and js2.files == run.manifest["files"]
+    for a, b in zip(served, run):
+        assert np.array_equal(a.step, b.step) and np.array_equal(a.time, b.time)
+        assert np.array_equal(a.positions, b.positions)
 
 
 def test_admission_waits_for_beads_and_rejects_beyond_the_queue():
