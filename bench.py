@@ -149,6 +149,8 @@ def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, boun
     with torch.cuda.stream(stream):
         ens = B.Ensemble([phys] * n, [sim] * n, Rs, [(1, -1, rank_seed0 + i) for i in range(n)], form=form)
         ens.ctx.set_bounds_refresh(bounds_every)
+        if form == "mixed":
+            ens.autotune(probe_steps=2)  # the team shape of the bucket (untimed, on copies of the state)
         t = 0.0
         for _ in range(warmup):
             ens.advance(t, CHUNK, CACHE_RESET_PER_CALL)
@@ -172,7 +174,8 @@ def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, boun
         failed = int(ens.failed().sum())
         obs = observables(ens, phys)
     delta = {k: c1[k] - c0[k] for k in c1}
-    return {"ms": times, "counters": delta, "failed": failed, "obs": obs}
+    shape = [(b["team_warps"], b["team_beads_per_thread"]) if b["kernel"] == 1 else (b["block"],) for b in ens.plan()]
+    return {"ms": times, "counters": delta, "failed": failed, "obs": obs, "shape": shape}
 
 
 def observables(ens, phys):
@@ -540,6 +543,7 @@ def main():
     print(json.dumps({"detail": "roofline", "flops_per_chain_step": fl_p, "dx_per_step_algorithm": dx_p,
                       "dx_per_step_mixed": dx_m, "fp32_fma_peak_tflops": peak32, "fp64_fma_peak_tflops": peak64,
                       "plain_tflops_dense_equiv": achieved_p, "plain_frac_of_fp64_peak": achieved_p / peak64,
+                      "mixed_team_shape_autotuned": mixed["shape"], "plain_block": plain["shape"],
                       "hbm_peak_gbs_measured": _peaks().get("hbm_gbs"),
                       "peak_source": "FMA-loop kernels (libbdsim_peak.so) timed in this run; the integrator runs "
                                      "on CUDA cores, neither HBM- nor tensor-bound"}))
