@@ -137,8 +137,12 @@ class Context:
         return [out[i].as_dict() for i in range(n.value)]
 
     def autotune(self, form, R, rng, cache, cache_valid, t_start, probe_steps: int = 3) -> list:
-        """Time the block-kernel launch shapes of each bucket on copies of the
-        given state and keep the fastest; returns the tuned plan."""
+        """Time every launch shape of each bucket (block kernel: block size,
+        Lanczos vectors and D in shared memory; team kernel: warps per chain
+        x beads per thread) on copies of the given state and keep the
+        fastest; returns the tuned plan. Probe from a warmed-up state (valid
+        warm-start cache): probes from a cold cache are dominated by the
+        first step's 30-step Lanczos run."""
         self.use_stream()
         self._ck(self.lib.bdcu_autotune(self.h, form_code(form), dptr(R), dptr(rng), dptr(cache),
                                         dptr(cache_valid), dptr(t_start), int(probe_steps)), "bdcu_autotune")
@@ -279,10 +283,14 @@ class Ensemble:
         """The launch plan of this ensemble's form: one dict per bucket."""
         return self.ctx.describe_plan(self.form)
 
-    def autotune(self, probe_steps: int = 3) -> list:
-        """Choose the block-kernel launch shape per bucket by timing each on a
-        copy of the current state (the state itself is not advanced)."""
-        self._t.copy_(self.torch.as_tensor(np.array([s.time_start for s in self.sims], dtype=np.float64)))
+    def autotune(self, probe_steps: int = 3, t_start=None) -> list:
+        """Choose the launch shape of each bucket (block kernel, and the
+        mixed form's team shape) by timing each on a copy of the current
+        state (the state itself is not advanced), from time t_start (per
+        chain or one value; default: each chain's SimParams.time_start).
+        Call it after a first chunk so that the probes start warm."""
+        t = [s.time_start for s in self.sims] if t_start is None else np.broadcast_to(t_start, (self.n,))
+        self._t.copy_(self.torch.as_tensor(np.array(t, dtype=np.float64)))
         return self.ctx.autotune(self.form, self.R, self.rng, self.cache, self.cache_valid, self._t, probe_steps)
 
     def reset_cache(self):

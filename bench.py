@@ -138,7 +138,7 @@ def flush_l2(torch, buf):
     buf.add_(1.0)  # a 256 MiB write, larger than the 126 MB L2
 
 
-def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, bounds_every=1):
+def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, bounds_every=1, team_shape=None):
     """Warm up, then time `steps` chunks with CUDA events on the launch stream.
     Each chunk starts its spectral (Lanczos) cache cold, as each integrate call
     of the reference's chunked simulate does. bounds_every: the mixed form's
@@ -149,12 +149,16 @@ def run_form(torch, form, Rs, phys, sim, steps, warmup, rank_seed0, stream, boun
     with torch.cuda.stream(stream):
         ens = B.Ensemble([phys] * n, [sim] * n, Rs, [(1, -1, rank_seed0 + i) for i in range(n)], form=form)
         ens.ctx.set_bounds_refresh(bounds_every)
-        if form == "mixed":
-            ens.autotune(probe_steps=2)  # the team shape of the bucket (untimed, on copies of the state)
+        if form == "mixed" and team_shape is not None:
+            ens.ctx.set_team_shape(0, *team_shape)
         t = 0.0
         for _ in range(warmup):
             ens.advance(t, CHUNK, CACHE_RESET_PER_CALL)
             t += CHUNK * DT
+        if form == "mixed" and team_shape is None:
+            # the bucket's team shape, timed on copies of the warmed-up state
+            # (warm spectral cache, as in every step of a chunk but the first)
+            ens.autotune(probe_steps=5, t_start=t)
         stream.synchronize()
         c0 = ens.counter_totals()
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -401,6 +405,8 @@ def main():
                     help="cfg2 (default): the headline line; others print their own line")
     ap.add_argument("--serving-seconds", type=float, default=60.0,
                     help="length of the serving replay (0: skip it)")
+    ap.add_argument("--team-shape", default=None,
+                    help="mixed form: pin the team shape 'warps,beads_per_thread' instead of autotuning (profiling)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -464,12 +470,13 @@ def main():
     results = {}
     clocks = None
     forms = [f for f in args.forms.split(",") if f]
+    shape = tuple(int(v) for v in args.team_shape.split(",")) if args.team_shape else None
     for form in forms:
         barrier()
         sampler = ClockSampler(local) if form == "mixed" else None
         if sampler:
             sampler.start()
-        r = run_form(torch, form, Rs, phys, sim, args.steps, args.warmup, first, stream)
+        r = run_form(torch, form, Rs, phys, sim, args.steps, args.warmup, first, stream, team_shape=shape)
         if sampler:
             clocks = sampler.stop()
         barrier()
@@ -479,7 +486,8 @@ def main():
     if set(forms) == {"plain", "mixed"}:
         # the persistent-bounds policy: spectral bounds kept for 4 steps
         barrier()
-        r = run_form(torch, "mixed", Rs, phys, sim, args.steps, args.warmup, first, stream, bounds_every=4)
+        r = run_form(torch, "mixed", Rs, phys, sim, args.steps, args.warmup, first, stream, bounds_every=4,
+                     team_shape=shape)
         barrier()
         r["total_ms"] = reduce_max(sum(r["ms"]), dist, device="cuda")
         results["mixed_k4"] = r
@@ -527,6 +535,7 @@ def main():
     if not args.no_cpu_baseline and world == 1:
         try:
             cpu = cpu_reference()
+            cpu.pop("wall_s", None)  # stated in the sample
         except Exception as exc:  # reported, not fatal
             cpu = {"error": str(exc)}
     ens_m = compare_observables(mixed["obs"], plain["obs"])
