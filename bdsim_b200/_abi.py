@@ -99,6 +99,44 @@ class BdcuBucketInfo(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BdcuQueueConfig(ctypes.Structure):
+    """bdcu_queue_config: the serving queue's pool and policy."""
+    _fields_ = [("form", ctypes.c_int32), ("policy", ctypes.c_int32), ("max_chains", ctypes.c_int32),
+                ("max_active_chains", ctypes.c_int32), ("bead_capacity", ctypes.c_int64),
+                ("arena_capacity", ctypes.c_int64), ("queue_limit", ctypes.c_int32), ("lookahead", ctypes.c_int32),
+                ("slice_steps", ctypes.c_int32), ("cache_mode", ctypes.c_int32), ("slice_budget_ns", ctypes.c_int64),
+                ("worker", ctypes.c_int32), ("reserved0", ctypes.c_int32)]
+
+
+class BdcuJob(ctypes.Structure):
+    """bdcu_job: one simulate call's chains for the serving queue."""
+    _fields_ = [("n_traj", ctypes.c_int32), ("snapshots", ctypes.c_int32), ("n_steps", ctypes.c_int64),
+                ("write_every", ctypes.c_int64), ("tag", ctypes.c_int64), ("phys", BdcuPhys), ("sim", BdcuSim),
+                ("arena", ctypes.POINTER(ctypes.c_double)), ("arena_len", ctypes.c_int64),
+                ("R0", ctypes.POINTER(ctypes.c_double)), ("rng", ctypes.POINTER(ctypes.c_int32))]
+
+
+class BdcuQueueEvent(ctypes.Structure):
+    """bdcu_queue_event: a snapshot, a completion or a rejection."""
+    _fields_ = [("kind", ctypes.c_int32), ("n_traj", ctypes.c_int32), ("n_beads", ctypes.c_int32),
+                ("snapshot", ctypes.c_int32), ("job", ctypes.c_int64), ("tag", ctypes.c_int64),
+                ("step", ctypes.c_int64), ("time", ctypes.c_double), ("t_arrival", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double), ("counters", BdcuCounters)]
+
+
+class BdcuQueueStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in (
+        "submitted", "rejected", "queued", "running", "done", "active_chains", "chain_steps", "slices",
+        "selected_chains", "pending_events")] + [("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+QUEUE_FIFO, QUEUE_SJF = 0, 1
+QEV_SNAPSHOT, QEV_DONE, QEV_REJECTED = 1, 2, 3
+
+
 class _Arena:
     def __init__(self):
         self.chunks = []
@@ -287,6 +325,20 @@ def load_library():
     lib.bdcu_set_single_launch.argtypes = [vp, ctypes.c_int]
     lib.bdcu_check_chains.argtypes = [ctypes.c_int, ctypes.POINTER(BdcuPhys), ctypes.POINTER(BdcuSim), c_double_p,
                                       ctypes.c_int64, ctypes.c_char_p, ctypes.c_int]
+    qp = ctypes.POINTER(BdcuQueueEvent)
+    lib.bdcu_queue_create.argtypes = [ctypes.c_int, ctypes.POINTER(BdcuQueueConfig), ctypes.POINTER(vp)]
+    lib.bdcu_queue_destroy.argtypes = [vp]
+    lib.bdcu_queue_last_error.argtypes = [vp]
+    lib.bdcu_queue_last_error.restype = ctypes.c_char_p
+    lib.bdcu_queue_submit.argtypes = [vp, ctypes.POINTER(BdcuJob), c_int64_p, ctypes.POINTER(ctypes.c_int)]
+    lib.bdcu_queue_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    lib.bdcu_queue_wait_idle.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
+    lib.bdcu_queue_poll.argtypes = [vp, qp, c_double_p, ctypes.c_int64, c_int32_p, ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_int)]
+    lib.bdcu_queue_get_stats.argtypes = [vp, ctypes.POINTER(BdcuQueueStats)]
+    for name in ("bdcu_queue_create", "bdcu_queue_destroy", "bdcu_queue_submit", "bdcu_queue_step",
+                 "bdcu_queue_wait_idle", "bdcu_queue_poll", "bdcu_queue_get_stats"):
+        getattr(lib, name).restype = ctypes.c_int
     for name in ("bdcu_set_single_launch", "bdcu_set_team_shape", "bdcu_check_chains", "bdcu_create", "bdcu_destroy", "bdcu_set_stream", "bdcu_set_chains",
                  "bdcu_count_steps", "bdcu_run", "bdcu_integrate_host", "bdcu_total_force",
                  "bdcu_forces", "bdcu_ran1", "bdcu_run_static", "bdcu_describe_plan", "bdcu_autotune",
@@ -303,6 +355,8 @@ EXPORTED_SYMBOLS = [
     "bdcu_total_force", "bdcu_forces", "bdcu_ran1", "bdcu_describe_plan", "bdcu_autotune",
     "bdcu_reserve", "bdcu_update_chains", "bdcu_write_arena", "bdcu_select", "bdcu_run_static",
     "bdcu_check_chains", "bdcu_set_team_shape", "bdcu_set_single_launch",
+    "bdcu_queue_create", "bdcu_queue_destroy", "bdcu_queue_last_error", "bdcu_queue_submit",
+    "bdcu_queue_step", "bdcu_queue_wait_idle", "bdcu_queue_poll", "bdcu_queue_get_stats",
 ]
 
 

@@ -1430,7 +1430,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 __syncthreads();
                 const double* xs[2] = {I, Fs};
                 double* ys[2] = {J, K};
-                B.apply_D_multi<2>(xs, ys);
+                B.template apply_D_multi<2>(xs, ys);
             }
             __syncthreads();
             for (int i = tid; i < n; i += blockDim.x) {
@@ -1484,7 +1484,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
             {
                 const double* xs[2] = {G, Fb};
                 double* ys[2] = {F, DFs};
-                B.apply_D_multi<2>(xs, ys);
+                B.template apply_D_multi<2>(xs, ys);
             }
             __syncthreads();
             for (int i = tid; i < n; i += blockDim.x) {

@@ -45,7 +45,7 @@ import numpy as np
 
 from ._abi import CACHE_PERSIST, CACHE_RESET_PER_CALL, COUNTER_FIELDS, ST_FATAL_MASK, count_steps
 from .engine import Context, _torch, form_code
-from . import storage
+from . import _abi, storage
 from .ensemble import INITIALIZERS, Initial, Output, _phys_summary, _segment, n_steps_of
 from .params import PhysParams, Rng, SimParams
 
@@ -538,3 +538,146 @@ class Server:
 
     def failed(self, js: JobState) -> np.ndarray:
         return (js.status & ST_FATAL_MASK) != 0
+
+
+class NativeQueue:
+    """The C ABI's serving queue (bdcu_queue_*, include/bdsim_cuda.h): the
+    policy of `Server` -- admission by slots, beads, arena and the active-chain
+    cap, FIFO with lookahead or shortest-job-first, one time-sliced launch per
+    iteration, a snapshot per chunk -- run by the native library, optionally
+    on its own worker thread, so that a C or C++ host serves the same way.
+    This class only packs `Job`s (initial positions from the job's
+    initializer, RNG states seed+i, one parameter record) and unpacks events.
+
+    Events (`poll`): dicts with kind "snapshot" (positions (n_traj, N, 3)),
+    "done" (status per chain, summed counters) or "rejected", and the job id,
+    tag, step, time and the queue-clock times of arrival, admission and
+    delivery."""
+
+    _KINDS = {_abi.QEV_SNAPSHOT: "snapshot", _abi.QEV_DONE: "done", _abi.QEV_REJECTED: "rejected"}
+
+    def __init__(self, device: int = 0, form="mixed", max_chains: int = 65536, bead_capacity: int = None,
+                 hbm_budget_bytes: int = 1 << 30, arena_capacity: int = 1 << 20, max_active_chains: int = None,
+                 queue_limit: int = None, lookahead: int = 16, cache_mode: int = CACHE_RESET_PER_CALL,
+                 slice_steps: int = 10, slice_budget_s: float = 1.0, policy: str = "fifo", worker: bool = False):
+        import ctypes
+        self._ct = ctypes
+        self.lib = _abi.load_library()
+        if policy not in ("fifo", "sjf"):
+            raise ValueError("policy is 'fifo' or 'sjf'")
+        cfg = _abi.BdcuQueueConfig()
+        cfg.form = form_code(form)
+        cfg.policy = _abi.QUEUE_FIFO if policy == "fifo" else _abi.QUEUE_SJF
+        cfg.max_chains = int(max_chains)
+        cfg.max_active_chains = int(max_active_chains or 0)
+        cfg.bead_capacity = int(bead_capacity or max(1024, hbm_budget_bytes // BYTES_PER_BEAD))
+        cfg.arena_capacity = int(arena_capacity)
+        cfg.queue_limit = int(queue_limit or 0)
+        cfg.lookahead = int(lookahead)
+        cfg.slice_steps = int(slice_steps)
+        cfg.cache_mode = int(cache_mode)
+        cfg.slice_budget_ns = int(slice_budget_s * 1e9)
+        cfg.worker = 1 if worker else 0
+        self.cfg = cfg
+        self.h = ctypes.c_void_p()
+        rc = self.lib.bdcu_queue_create(int(device), ctypes.byref(cfg), ctypes.byref(self.h))
+        if rc != 0:
+            raise RuntimeError(f"bdcu_queue_create failed ({rc}): {self.lib.bdcu_queue_last_error(None).decode()}")
+        self._pos = np.zeros(0, dtype=np.float64)
+        self._status = np.zeros(cfg.max_chains, dtype=np.int32)
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc}): {self.lib.bdcu_queue_last_error(self.h).decode()}")
+
+    def close(self):
+        if self.h:
+            self.lib.bdcu_queue_destroy(self.h)
+            self.h = self._ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, job: Job, tag: int = 0, snapshots: bool = None):
+        """Queue a job; returns (job id, accepted). snapshots: deliver every
+        chunk (default: job.keep_snapshots) or only the final positions."""
+        ct = self._ct
+        N, n = int(job.phys.number_of_beads), int(job.n_traj)
+        init = job.initial or Initial()
+        R0 = np.ascontiguousarray(np.concatenate(
+            [INITIALIZERS[init.method](N, job.seed + t, dict(init.kwargs)) for t in range(n)]).reshape(-1, 3),
+            dtype=np.float64)
+        rng = np.ascontiguousarray([Rng(job.seed + t).state() for t in range(n)], dtype=np.int32)
+        prec, srec, arena = _abi.pack_batch([job.phys], [job.sim], [N])
+        d = _abi.BdcuJob()
+        d.n_traj = n
+        d.snapshots = int(job.keep_snapshots if snapshots is None else snapshots)
+        d.n_steps = int(job.n_steps) if job.n_steps is not None else n_steps_of(job.sim)
+        d.write_every = int(job.write_every) if job.write_every and job.write_every > 0 else 0
+        d.tag = int(tag)
+        d.phys = prec[0]
+        d.sim = srec[0]
+        r = prec[0]
+        uses = r.phi_offset >= 0 or r.flow_n_times > 0 or r.ext_n_entries > 0
+        arena = np.ascontiguousarray(arena if uses else np.zeros(0), dtype=np.float64)
+        d.arena = arena.ctypes.data_as(_abi.c_double_p) if arena.size else None
+        d.arena_len = int(arena.size)
+        d.R0 = R0.ctypes.data_as(_abi.c_double_p)
+        d.rng = rng.ctypes.data_as(_abi.c_int32_p)
+        jid, ok = ct.c_int64(0), ct.c_int(0)
+        self._ck(self.lib.bdcu_queue_submit(self.h, ct.byref(d), ct.byref(jid), ct.byref(ok)), "bdcu_queue_submit")
+        return int(jid.value), bool(ok.value)
+
+    def step(self) -> bool:
+        """One iteration (caller-driven queues); True while jobs remain."""
+        busy = self._ct.c_int(0)
+        self._ck(self.lib.bdcu_queue_step(self.h, self._ct.byref(busy)), "bdcu_queue_step")
+        return bool(busy.value)
+
+    def wait_idle(self, timeout_s: float = None) -> bool:
+        """Run (or wait for the worker) until no job is queued or running;
+        returns True if jobs remain at the timeout."""
+        busy = self._ct.c_int(0)
+        ms = -1 if timeout_s is None else int(timeout_s * 1000)
+        self._ck(self.lib.bdcu_queue_wait_idle(self.h, ms, self._ct.byref(busy)), "bdcu_queue_wait_idle")
+        return bool(busy.value)
+
+    def poll(self):
+        """The oldest undelivered event as a dict, or None."""
+        ct = self._ct
+        ev, got = _abi.BdcuQueueEvent(), ct.c_int(0)
+        while True:
+            rc = self.lib.bdcu_queue_poll(self.h, ct.byref(ev), self._pos.ctypes.data_as(_abi.c_double_p),
+                                          self._pos.size, self._status.ctypes.data_as(_abi.c_int32_p),
+                                          self._status.size, ct.byref(got))
+            if rc == 5:  # BDCU_E_LIMIT: the positions buffer is too small for this event
+                self._pos = np.zeros(3 * ev.n_traj * ev.n_beads, dtype=np.float64)
+                continue
+            self._ck(rc, "bdcu_queue_poll")
+            break
+        if not got.value:
+            return None
+        out = {"kind": self._KINDS[ev.kind], "job": ev.job, "tag": ev.tag, "n_traj": ev.n_traj,
+               "n_beads": ev.n_beads, "step": ev.step, "time": ev.time, "t_arrival": ev.t_arrival,
+               "t_admit": ev.t_admit, "t_done": ev.t_done}
+        if ev.kind == _abi.QEV_SNAPSHOT:
+            out["snapshot"] = ev.snapshot
+            out["positions"] = self._pos[:3 * ev.n_traj * ev.n_beads].reshape(ev.n_traj, ev.n_beads, 3).copy()
+        elif ev.kind == _abi.QEV_DONE:
+            out["status"] = self._status[:ev.n_traj].copy()
+            out["counters"] = {f: getattr(ev.counters, f) for f in COUNTER_FIELDS}
+        return out
+
+    def events(self) -> list:
+        out = []
+        while (e := self.poll()) is not None:
+            out.append(e)
+        return out
+
+    def stats(self) -> dict:
+        st = _abi.BdcuQueueStats()
+        self._ck(self.lib.bdcu_queue_get_stats(self.h, self._ct.byref(st)), "bdcu_queue_get_stats")
+        return st.as_dict()

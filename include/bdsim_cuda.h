@@ -25,6 +25,8 @@
  *   bdcu_set_chains       PhysParams / SimParams marshalling
  *                         (src/model.hpp:20-35, src/integrator.hpp:22-28,
  *                         pickled state tuples bindings/module.cpp:184-297)
+ *   bdcu_queue_*          many simulate calls (python/bdsim/ensemble.py:179-227)
+ *                         served concurrently from one slot pool
  *
  * Parameter layout. One bdcu_phys and one bdcu_sim per chain. Variable-size
  * tables (flow samples, external-force samples, SDK phi) live in one double
@@ -389,6 +391,122 @@ int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phys, const bd
                     const double* arena, int64_t arena_len, double* R, int32_t* rng, double* cache,
                     int32_t* cache_valid, const double* t_start, const int32_t* n_steps, int32_t* status,
                     bdcu_counters* counters, int form, int cache_mode);
+
+/* ---- Serving queue: continuous batching of ensemble jobs on one GPU, for a
+   host that is not Python (no counterpart in the reference, whose simulate
+   runs one ensemble per call to completion, python/bdsim/ensemble.py:179-227).
+   A job is the arguments of one simulate call: n_traj chains of one
+   bdcu_phys/bdcu_sim record, their initial positions and RNG states, the total
+   steps and the snapshot interval. The queue owns a slot pool (bdcu_reserve)
+   and its state buffers on the device and runs the policy of the Python
+   bdsim_b200.serving.Server:
+   - admission: a job needs n_traj consecutive slots, n_traj*N consecutive
+     beads, room for its tables in the arena and room under the active-chain
+     cap; queued jobs are admitted first-fit in arrival order over a lookahead
+     window (BDCU_QUEUE_FIFO) or smallest n_traj*n_steps*N^2 first
+     (BDCU_QUEUE_SJF); submissions beyond queue_limit queued jobs, or larger
+     than the pool, are rejected;
+   - each iteration is one bdcu_run_slice over the chains of every running
+     job: each takes up to slice_steps steps of its current chunk
+     (write_every steps, the job's snapshot interval) and none starts a step
+     after slice_budget_ns;
+   - a chunk of k steps is one integrate span [t0, t0+(k-1)dt] with
+     t0 = time_start + step*dt, started with a cold spectral cache under
+     BDCU_CACHE_RESET_PER_CALL (the reference's per-call semantics) and
+     continued across slices with its cache, so a job's positions equal,
+     bit for bit, those of integrating its chains chunk by chunk;
+   - when every chain of a job has finished a chunk its positions are copied
+     to the host as a snapshot event; after the last chunk (or once every
+     chain has a fatal status) a DONE event carries the statuses and the
+     summed counters, and the job's slots are freed.
+   Threading: with cfg.worker = 1 a library thread drives the queue and
+   submit / poll / stats / wait_idle may be called from any thread; with
+   worker = 0 the caller drives it with bdcu_queue_step (or wait_idle) from one
+   thread, and the other entry points may still be called from any thread. */
+typedef struct bdcu_queue bdcu_queue;
+enum { BDCU_QUEUE_FIFO = 0, BDCU_QUEUE_SJF = 1 };
+typedef struct bdcu_queue_config {
+    int32_t form;               /* BDCU_FORM_* */
+    int32_t policy;             /* BDCU_QUEUE_FIFO | BDCU_QUEUE_SJF */
+    int32_t max_chains;         /* chain slots of the pool (>= 1) */
+    int32_t max_active_chains;  /* cap on running chains (0: max_chains) */
+    int64_t bead_capacity;      /* beads of the pool (>= 2) */
+    int64_t arena_capacity;     /* doubles for the jobs' tables (>= 0) */
+    int32_t queue_limit;        /* queued jobs beyond which submit rejects (0: no limit) */
+    int32_t lookahead;          /* FIFO: queued jobs examined per admission (0: 16) */
+    int32_t slice_steps;        /* steps per chain per iteration (>= 1) */
+    int32_t cache_mode;         /* BDCU_CACHE_* at each chunk start */
+    int64_t slice_budget_ns;    /* no chain starts a step after this (0: no limit) */
+    int32_t worker;             /* 1: a library thread drives the queue */
+    int32_t reserved0;
+} bdcu_queue_config;
+typedef struct bdcu_job {
+    int32_t n_traj;             /* chains */
+    int32_t snapshots;          /* 1: an event per chunk (and the initial state); 0: the final one */
+    int64_t n_steps;            /* steps of the whole job (>= 0) */
+    int64_t write_every;        /* steps per chunk (0: one chunk) */
+    int64_t tag;                /* the caller's id, echoed in the job's events */
+    bdcu_phys phys;             /* every chain's record; table offsets index `arena` */
+    bdcu_sim sim;               /* dt, tolerance, centre-of-mass flag, time_start */
+    const double* arena;        /* the job's tables (host; may be NULL when arena_len = 0) */
+    int64_t arena_len;
+    const double* R0;           /* n_traj * n_beads * 3 doubles (host) */
+    const int32_t* rng;         /* n_traj * 3 int32: (ix, iy, seed) per chain (host) */
+} bdcu_job;
+enum { BDCU_QEV_SNAPSHOT = 1, BDCU_QEV_DONE = 2, BDCU_QEV_REJECTED = 3 };
+typedef struct bdcu_queue_event {
+    int32_t kind;               /* BDCU_QEV_* */
+    int32_t n_traj;
+    int32_t n_beads;
+    int32_t snapshot;           /* SNAPSHOT: index (0 = the initial state) */
+    int64_t job;                /* id from bdcu_queue_submit */
+    int64_t tag;
+    int64_t step;               /* steps completed at this event */
+    double time;                /* SNAPSHOT: time of the positions (time_start + step*dt) */
+    double t_arrival;           /* seconds since the queue was created */
+    double t_admit;             /* (< 0: not admitted) */
+    double t_done;              /* DONE: delivery of the last snapshot */
+    bdcu_counters counters;     /* DONE: summed over the job's chains */
+} bdcu_queue_event;
+typedef struct bdcu_queue_stats {
+    int64_t submitted, rejected, queued, running, done;
+    int64_t active_chains;
+    int64_t chain_steps;        /* steps completed by all chains */
+    int64_t slices;             /* bdcu_run_slice launches */
+    int64_t selected_chains;    /* sum over slices of the chains advanced */
+    int64_t pending_events;
+    double device_ms;           /* device time of the slice launches */
+} bdcu_queue_stats;
+/* Allocates the pool's device buffers (R and warm-start vectors of
+   bead_capacity*3 doubles, per-slot RNG, status, counters and step arrays)
+   and a context; starts the worker thread when cfg->worker = 1. */
+int bdcu_queue_create(int device, const bdcu_queue_config* cfg, bdcu_queue** out);
+/* Stops the worker (after its current iteration) and frees everything;
+   undelivered events are dropped. */
+int bdcu_queue_destroy(bdcu_queue* q);
+const char* bdcu_queue_last_error(bdcu_queue* q);
+/* Copies the job (records, tables, R0, rng) and queues it, or rejects it
+   (*accepted = 0, and a REJECTED event) when queue_limit jobs are queued or
+   the job is larger than the pool. Records get the checks of bdcu_check_chains
+   against the job's own arena: a failing record returns its BDCU_E_* code and
+   queues nothing. *job_id receives the job's id either way. */
+int bdcu_queue_submit(bdcu_queue* q, const bdcu_job* job, int64_t* job_id, int* accepted);
+/* Caller-driven mode: one iteration (admission, one slice launch, waiting
+   for it, the events of the chunks it completed). *busy = 1 while jobs are
+   queued or running. BDCU_E_STATE in worker mode. */
+int bdcu_queue_step(bdcu_queue* q, int* busy);
+/* Until no job is queued or running, or timeout_ms passes (< 0: no limit):
+   waits for the worker, or in caller-driven mode runs iterations. *busy as in
+   bdcu_queue_step. */
+int bdcu_queue_wait_idle(bdcu_queue* q, int64_t timeout_ms, int* busy);
+/* Takes the oldest undelivered event (*got = 1; 0 when there is none).
+   SNAPSHOT events copy n_traj*n_beads*3 doubles into positions and DONE
+   events n_traj statuses into status; a buffer that is NULL is skipped, one
+   that is too small returns BDCU_E_LIMIT with *ev filled in and the event
+   kept, so the caller can size its buffers from ev and poll again. */
+int bdcu_queue_poll(bdcu_queue* q, bdcu_queue_event* ev, double* positions, int64_t positions_len,
+                    int32_t* status, int32_t status_len, int* got);
+int bdcu_queue_get_stats(bdcu_queue* q, bdcu_queue_stats* out);
 
 #ifdef __cplusplus
 }

@@ -63,7 +63,9 @@ def test_abi_struct_layout_matches_header(tmp_path):
         pytest.skip("no C compiler")
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bdsim_cuda.h"', "int main(void) {"]
     for cname, cls in (("bdcu_phys", _abi.BdcuPhys), ("bdcu_sim", _abi.BdcuSim), ("bdcu_counters", _abi.BdcuCounters),
-                       ("bdcu_bucket_info", _abi.BdcuBucketInfo)):
+                       ("bdcu_bucket_info", _abi.BdcuBucketInfo), ("bdcu_queue_config", _abi.BdcuQueueConfig),
+                       ("bdcu_job", _abi.BdcuJob), ("bdcu_queue_event", _abi.BdcuQueueEvent),
+                       ("bdcu_queue_stats", _abi.BdcuQueueStats)):
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for fname, _ in cls._fields_:
             lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
@@ -75,7 +77,9 @@ def test_abi_struct_layout_matches_header(tmp_path):
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
     c_layout = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
     for cname, cls in (("bdcu_phys", _abi.BdcuPhys), ("bdcu_sim", _abi.BdcuSim), ("bdcu_counters", _abi.BdcuCounters),
-                       ("bdcu_bucket_info", _abi.BdcuBucketInfo)):
+                       ("bdcu_bucket_info", _abi.BdcuBucketInfo), ("bdcu_queue_config", _abi.BdcuQueueConfig),
+                       ("bdcu_job", _abi.BdcuJob), ("bdcu_queue_event", _abi.BdcuQueueEvent),
+                       ("bdcu_queue_stats", _abi.BdcuQueueStats)):
         assert c_layout[(cname, "size")] == ctypes.sizeof(cls)
         for fname, _ in cls._fields_:
             assert c_layout[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
@@ -189,3 +193,51 @@ def test_check_chains_rejects_negative_flow_offset_and_bead_limit():
     prec[0].n_beads = 5000
     rc, msg = _abi.check_records(1, prec, srec, arena)
     assert rc == 5 and "n_beads" in msg
+
+
+def _queue_config(**kw):
+    cfg = _abi.BdcuQueueConfig()
+    cfg.form, cfg.policy, cfg.max_chains, cfg.bead_capacity = 1, _abi.QUEUE_FIFO, 8, 256
+    cfg.arena_capacity, cfg.slice_steps, cfg.cache_mode = 64, 10, _abi.CACHE_RESET_PER_CALL
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+@pytest.mark.parametrize("bad", [dict(form=7), dict(policy=2), dict(max_chains=0), dict(bead_capacity=1),
+                                 dict(arena_capacity=-1), dict(queue_limit=-1), dict(slice_steps=0),
+                                 dict(cache_mode=9), dict(slice_budget_ns=-5), dict(worker=2)])
+def test_queue_config_checks_come_before_the_gpu(bad):
+    """bdcu_queue_create rejects a bad configuration with BDCU_E_ARG and a
+    message before it touches CUDA."""
+    lib = _abi.load_library()
+    h = ctypes.c_void_p()
+    cfg = _queue_config(**bad)
+    assert lib.bdcu_queue_create(0, ctypes.byref(cfg), ctypes.byref(h)) == 1
+    assert not h.value
+    assert lib.bdcu_queue_last_error(None).decode()
+
+
+def test_queue_entry_points_reject_null_handles():
+    lib = _abi.load_library()
+    ev, got, busy = _abi.BdcuQueueEvent(), ctypes.c_int(), ctypes.c_int()
+    jid, ok = ctypes.c_int64(), ctypes.c_int()
+    st = _abi.BdcuQueueStats()
+    assert lib.bdcu_queue_submit(None, None, ctypes.byref(jid), ctypes.byref(ok)) == 1
+    assert lib.bdcu_queue_step(None, ctypes.byref(busy)) == 1
+    assert lib.bdcu_queue_wait_idle(None, 0, ctypes.byref(busy)) == 1
+    assert lib.bdcu_queue_poll(None, ctypes.byref(ev), None, 0, None, 0, ctypes.byref(got)) == 1
+    assert lib.bdcu_queue_get_stats(None, ctypes.byref(st)) == 1
+    assert lib.bdcu_queue_destroy(None) == 1
+    assert lib.bdcu_queue_create(0, None, None) == 1
+
+
+def test_queue_create_without_a_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = _abi.load_library()
+    h = ctypes.c_void_p()
+    cfg = _queue_config()
+    assert lib.bdcu_queue_create(0, ctypes.byref(cfg), ctypes.byref(h)) == 2  # BDCU_E_CUDA
+    assert not h.value and lib.bdcu_queue_last_error(None).decode()
