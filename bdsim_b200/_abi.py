@@ -23,7 +23,8 @@ ST_CHEB_FALLBACK = 4
 ST_RTSAFE_FAIL = 8
 ST_NONFINITE = 16
 ST_BAD_PARAM = 32
-ST_FATAL_MASK = ST_NOT_PD | ST_RTSAFE_FAIL | ST_NONFINITE | ST_BAD_PARAM
+ST_TIMEOUT = 64
+ST_FATAL_MASK = ST_NOT_PD | ST_RTSAFE_FAIL | ST_NONFINITE | ST_BAD_PARAM | ST_TIMEOUT
 
 FORM_PLAIN_FP64 = 0
 FORM_MIXED_FP32 = 1
@@ -37,6 +38,7 @@ STATUS_NAMES = {
     ST_RTSAFE_FAIL: "rtsafe failed (root not bracketed or max iterations)",
     ST_NONFINITE: "bead positions became non-finite",
     ST_BAD_PARAM: "invalid parameter (WLCbounded sigma > 1 or ExactSqrt)",
+    ST_TIMEOUT: "a bounded wait inside the kernel gave up (tile staging)",
 }
 
 

@@ -33,7 +33,7 @@ constexpr int kCoefCap = 504;  // >= kMaxCheb + 1
 // slots kCholFirstSlot.. (free while D is factored).
 constexpr int kBlockedCholMin = 300;
 constexpr int kCholTile = 64;
-constexpr int kCholTileStride = kCholTile + 8;
+constexpr int kCholTileStride = kCholTile + 4;
 constexpr int kCholMaxPanel = 32;
 constexpr int kCholMaxBlock = 64;
 constexpr int kCholFirstSlot = 7;
@@ -76,6 +76,12 @@ __host__ __device__ inline SmemLayout smem_layout(int n_max, int d_in_smem, int 
     return s;
 }
 
+// Leading dimension of the Cholesky factor Lt (column k of L at Lt + k*ld):
+// n rounded up to 16 doubles, so that every column, and every 64-row segment
+// of it starting at a multiple of 8 rows, begins on a 128-byte line (the
+// bulk copies of the blocked factorisation need 16-byte alignment).
+__host__ __device__ inline int chol_ld(int n) { return (n + 15) / 16 * 16; }
+
 // Global scratch per thread block (doubles): dense D when it is not in shared
 // memory (plain form), the Cholesky factor, and the cold Lanczos basis.
 struct ScratchLayout {
@@ -89,7 +95,7 @@ __host__ __device__ inline ScratchLayout scratch_layout(int n_max, int d_in_smem
     int64_t o = 0;
     const int64_t nn = (int64_t)n_max * n_max, nn16 = (nn + 15) / 16 * 16;
     s.D = o;  if (!mixed && need_d && !d_in_smem) o += nn16;
-    s.Lt = o; if (need_chol) o += nn16;
+    s.Lt = o; if (need_chol) o += (int64_t)n_max * chol_ld(n_max);
     s.V = o;  if (need_lz && v_cap < kLanczosCold) o += ((int64_t)kLanczosCold * round_up8(n_max) + 15) / 16 * 16;
     s.total = o;
     return s;
@@ -276,7 +282,8 @@ struct Block {
     double* Vg;        // global Lanczos basis (kLanczosCold vectors)
     double* D;         // plain: dense D (shared or global)
     int ldd;
-    double* Lt;        // transposed Cholesky factor, global scratch (ld = n)
+    double* Lt;        // transposed Cholesky factor, global scratch (leading dimension ldl)
+    int ldl;           // chol_ld(n)
     double* stage;     // blocked Cholesky tile staging (vector slots kCholFirstSlot..)
     int64_t stage_cap; // doubles available at stage
     float4* pos32;     // mixed: FP32 bead coordinates
@@ -416,7 +423,7 @@ struct Block {
     }
 
     // ---- Cholesky (cholesky_lower, src/linalg.cpp:91-107) ---------------
-    // Right-looking on Lt = L^T (Lt[k*n + i] = L(i,k)). Element (i,j) receives
+    // Right-looking on Lt = L^T (Lt[k*ldl + i] = L(i,k)). Element (i,j) receives
     // M(i,j) - L(i,0)L(j,0) - L(i,1)L(j,1) - ... in k order, then / L(j,j):
     // the reference's rounding sequence. Returns false on a pivot <= 0.
     // src: dense D at (Dp, ld) or, if src_in_lt, Lt already holds D's lower part.
@@ -426,26 +433,26 @@ struct Block {
         double* L = Lt;
         if (!src_in_lt) {
             for (int j = threadIdx.x >> 5; j < n; j += blockDim.x >> 5)
-                for (int i = j + (threadIdx.x & 31); i < n; i += 32) L[(int64_t)j * n + i] = Dp[(int64_t)i * ld + j];
+                for (int i = j + (threadIdx.x & 31); i < n; i += 32) L[(int64_t)j * ldl + i] = Dp[(int64_t)i * ld + j];
         }
         __syncthreads();
         const int nb = chol_panel_width();
         if (nb > 0) return cholesky_blocked(nb);
         for (int k = 0; k < n; ++k) {
             if (threadIdx.x == 0) {
-                const double s = L[(int64_t)k * n + k];
-                if (!(s > 0.0)) ctl.brk = 1; else L[(int64_t)k * n + k] = sqrt(s);
+                const double s = L[(int64_t)k * ldl + k];
+                if (!(s > 0.0)) ctl.brk = 1; else L[(int64_t)k * ldl + k] = sqrt(s);
             }
             __syncthreads();
             if (ctl.brk) return false;
-            const double dk = L[(int64_t)k * n + k];
-            for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) L[(int64_t)k * n + i] = L[(int64_t)k * n + i] / dk;
+            const double dk = L[(int64_t)k * ldl + k];
+            for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) L[(int64_t)k * ldl + i] = L[(int64_t)k * ldl + i] / dk;
             __syncthreads();
-            const double* colk = L + (int64_t)k * n;
+            const double* colk = L + (int64_t)k * ldl;
             for (int j = k + 1 + (threadIdx.x >> 5); j < n; j += blockDim.x >> 5) {
                 const double ljk = colk[j];
                 for (int i = j + (threadIdx.x & 31); i < n; i += 32)
-                    L[(int64_t)j * n + i] = L[(int64_t)j * n + i] - colk[i] * ljk;
+                    L[(int64_t)j * ldl + i] = L[(int64_t)j * ldl + i] - colk[i] * ljk;
             }
             __syncthreads();
         }
@@ -487,10 +494,12 @@ struct Block {
             for (int p0 = kb; p0 < ke; p0 += kCholMaxPanel) {
                 const int p1 = p0 + kCholMaxPanel < ke ? p0 + kCholMaxPanel : ke;
                 if (p0 > kb) chol_update(kb, p0, p0, p0, p1);
+                if (ctl.brk) return false;  // a staging wait expired
                 if (!chol_panel(p0, p1)) return false;
             }
             if (ke >= n) break;
             chol_update(kb, ke, ke, ke, n);
+            if (ctl.brk) return false;
         }
         return true;
     }
@@ -500,6 +509,11 @@ struct Block {
     __device__ void chol_update(int k0, int k1, int r0, int c0, int c1) {
         double* L = Lt;
         const int kk = k1 - k0, kk4 = (kk + 3) & ~3;  // staged rows k >= kk are zero
+        if constexpr (kMixed)
+            if ((int64_t)kStageBufs * kk4 * kCholTileStride + 8 <= stage_cap && (r0 & 7) == 0 && (c0 & 7) == 0) {
+                chol_update_bulk(k0, k1, r0, c0, c1);
+                return;
+            }
         if constexpr (!kMixed)
             if (blockDim.x == 512 && (int64_t)3 * kk4 * kCholTile <= stage_cap) {
                 chol_update_pairs(k0, k1, r0, c0, c1);
@@ -536,8 +550,8 @@ struct Block {
                     for (int u = 0; u < kStageBatch; ++u) {
                         const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
                         const bool kin = e < tot && k < kk;
-                        va[u] = (stA && kin && i0 + r < n) ? L[(int64_t)(k0 + k) * n + i0 + r] : 0.0;
-                        vb[u] = (stB && kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * n + j0 + r] : 0.0;
+                        va[u] = (stA && kin && i0 + r < n) ? L[(int64_t)(k0 + k) * ldl + i0 + r] : 0.0;
+                        vb[u] = (stB && kin && j0 + r < c1) ? L[(int64_t)(k0 + k) * ldl + j0 + r] : 0.0;
                     }
 #pragma unroll
                     for (int u = 0; u < kStageBatch; ++u) {
@@ -562,6 +576,195 @@ struct Block {
             else chol_tile_dmma(As, Bt, i0, j0, c1, kk4, warp, lane, nwarps);
             __syncthreads();
         }
+    }
+
+    // chol_update for the mixed form with its panel rows staged by bulk
+    // copies (cp.async.bulk, global -> shared, completion on an mbarrier)
+    // issued one tile ahead. The panel rows L(x + r, k0 + k), r < kCholTile,
+    // k < kk, of the tile row or tile column starting at row x are the same
+    // data whether a tile uses them as A (i0 = x) or as B (j0 = x), so
+    // kStageBufs buffers form a pool tagged by x. Before tile t is multiplied,
+    // the rows tile t + 1 needs and the pool lacks are requested into buffers
+    // tile t does not use, and tile t + 1's C columns are prefetched into L2
+    // (cp.async.bulk.prefetch.L2); a tile row ends with its diagonal tile,
+    // which uses one buffer, so the next row's A and B both arrive ahead.
+    // There is no block barrier between tiles: warp 0 issues the copies
+    // (lane 0 posts the byte count on the buffer's "full" mbarrier), every
+    // warp waits on "full" before reading a buffer and, after the last tile
+    // that uses it, arrives on its "empty" mbarrier (one arrival per warp);
+    // warp 0 waits on "empty" before refilling a buffer. Column k of L
+    // starts at Lt + k*ldl (a multiple of 16 doubles) and x is a multiple of 8,
+    // so each copy is min(kCholTile, ldl - x) doubles on 16-byte boundaries;
+    // rows beyond n or c1 in a buffer (padding, stale data) reach only C rows
+    // or columns that are not stored, and rows k in [kk, kk4) are zero. The
+    // panel columns are not written during the update; the generic-proxy
+    // writes that produced them are ordered before the copies by a barrier and
+    // fence.proxy.async. Every wait is bounded: on expiry the block records
+    // ctl.brk = 2, waits (bounded) for its copies in flight and returns.
+    static constexpr int kStageBufs = 3;
+
+    __device__ __forceinline__ static uint32_t smem_addr(const void* p) {
+        return (uint32_t)__cvta_generic_to_shared(p);
+    }
+
+    // Warp 0: the copies of panel rows starting at x into buf, completing on
+    // bar (lane 0 posts the byte count, then each lane issues every 32nd row).
+    __device__ void bulk_stage(double* buf, uint64_t* bar, int k0, int kk, int x, int lane) const {
+        const int cnt = ldl - x < kCholTile ? ldl - x : kCholTile;
+        const uint32_t bytes = (uint32_t)cnt * 8u, mb = smem_addr(bar);
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes * (uint32_t)kk)
+                         : "memory");
+        __syncwarp();
+        for (int k = lane; k < kk; k += 32) {
+            const double* src = Lt + (int64_t)(k0 + k) * ldl + x;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_addr(buf + k * kCholTileStride)),
+                         "l"(src), "r"(bytes), "r"(mb)
+                         : "memory");
+        }
+    }
+
+    // Wait for phase `parity` of bar; false if the bounded wait expired.
+    __device__ static bool bar_wait(uint64_t* bar, uint32_t parity) {
+        const uint32_t mb = smem_addr(bar);
+        for (int it = 0; it < (1 << 20); ++it) {
+            uint32_t done;
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                : "=r"(done)
+                : "r"(mb), "r"(parity)
+                : "memory");
+            if (done) return true;
+        }
+        return false;
+    }
+
+    __device__ void chol_update_bulk(int k0, int k1, int r0, int c0, int c1) {
+        const int kk = k1 - k0, kk4 = (kk + 3) & ~3;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+        const int nti = (n - r0 + kCholTile - 1) / kCholTile, ntj = (c1 - c0 + kCholTile - 1) / kCholTile;
+        const int nt = nti * ntj;
+        const int64_t bstride = (int64_t)kk4 * kCholTileStride;
+        uint64_t* full = reinterpret_cast<uint64_t*>(stage + stage_cap - 8);  // copies landed
+        uint64_t* empty = full + kStageBufs;                                   // every warp done reading
+        for (int e = threadIdx.x; e < kStageBufs * (kk4 - kk) * kCholTile; e += blockDim.x) {
+            const int b = e / ((kk4 - kk) * kCholTile), rem = e % ((kk4 - kk) * kCholTile);
+            stage[b * bstride + (kk + rem / kCholTile) * kCholTileStride + rem % kCholTile] = 0.0;
+        }
+        if (threadIdx.x == 0)
+            for (int b = 0; b < kStageBufs; ++b) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(full + b)) : "memory");
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(empty + b)), "r"(nwarps)
+                             : "memory");
+            }
+        if (warp == 0) {  // the issuing warp: barrier inits visible, panel writes ordered before the copies
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async;" ::: "memory");
+        }
+        __syncthreads();
+        // Pool state, the same in every warp: the row each buffer holds or is
+        // receiving (-1: none), a fill not yet consumed, a release the issuing
+        // warp has not yet waited for, and the two barriers' phase parities.
+        // A buffer released after its last use gives up its row (it is
+        // fetched again if needed), so each release pairs with the next fill.
+        int tag[kStageBufs], pend[kStageBufs], rel[kStageBufs];
+        uint32_t par[kStageBufs], epar[kStageBufs];
+#pragma unroll
+        for (int b = 0; b < kStageBufs; ++b) tag[b] = -1, pend[b] = 0, rel[b] = 0, par[b] = 0, epar[b] = 0;
+        volatile int32_t* gave_up = &ctl.brk;
+        auto next_tile = [&](int t) {  // first tile >= t not wholly above the diagonal
+            while (t < nt && r0 + (t / ntj) * kCholTile + kCholTile - 1 < c0 + (t % ntj) * kCholTile) ++t;
+            return t;
+        };
+        auto find = [&](int x) {
+            int f = -1;
+#pragma unroll
+            for (int b = 0; b < kStageBufs; ++b)
+                if (tag[b] == x) f = b;
+            return f;
+        };
+        // request row x unless present, into a buffer whose row is none of
+        // keep0..keep2 (-2: no row) (no buffer free: it is requested again
+        // when its tile comes); the issuing warp first waits until every warp
+        // has released the buffer's previous contents
+        auto request = [&](int x, int keep0, int keep1, int keep2) {
+            if (find(x) >= 0) return;
+            int f = -1;
+#pragma unroll
+            for (int b = kStageBufs - 1; b >= 0; --b)
+                if (tag[b] != keep0 && tag[b] != keep1 && tag[b] != keep2) f = b;
+            if (f < 0) return;
+#pragma unroll
+            for (int b = 0; b < kStageBufs; ++b)
+                if (b == f) {
+                    if (warp == 0) {
+                        const bool freed = !rel[b] || __all_sync(0xffffffffu, bar_wait(empty + b, epar[b]));
+                        if (freed) bulk_stage(stage + b * bstride, full + b, k0, kk, x, lane);
+                        else if (lane == 0) *gave_up = 2;
+                    }
+                    if (rel[b]) epar[b] ^= 1u, rel[b] = 0;
+                    tag[b] = x, pend[b] = 1;
+                }
+        };
+        for (int t = next_tile(0), tn; t < nt; t = tn) {
+            if (*gave_up) break;
+            const int i0 = r0 + (t / ntj) * kCholTile, j0 = c0 + (t % ntj) * kCholTile;
+            request(i0, i0, j0, -2);  // (present after a prefetch; else fetched now)
+            request(j0, i0, j0, -2);
+            const int ba = find(i0), bb = find(j0);
+            bool landed = true;
+#pragma unroll
+            for (int b = 0; b < kStageBufs; ++b)
+                if (pend[b] && (b == ba || b == bb)) {
+                    if (__all_sync(0xffffffffu, bar_wait(full + b, par[b])))
+                        par[b] ^= 1u, pend[b] = 0;
+                    else
+                        landed = false;
+                }
+            if (!landed) {
+                if (lane == 0) *gave_up = 2;
+                break;
+            }
+            tn = next_tile(t + 1);
+            const int i1 = tn < nt ? r0 + (tn / ntj) * kCholTile : -2, j1 = tn < nt ? c0 + (tn % ntj) * kCholTile : -2;
+            if (tn < nt) {  // the next tile's rows into buffers this tile does not use
+                request(i1, i0, j0, -2);
+                request(j1, i0, j0, i1);
+                // and its C columns into L2 (bulk prefetch, one per column segment)
+                if (warp == 1 % nwarps) {
+                    const int cnt = ldl - i1 < kCholTile ? ldl - i1 : kCholTile;
+                    const int jn = c1 - j1 < kCholTile ? c1 - j1 : kCholTile;
+                    for (int c = lane; c < jn; c += 32)
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Lt + (int64_t)(j1 + c) * ldl + i1),
+                                     "r"((uint32_t)cnt * 8u)
+                                     : "memory");
+                }
+            }
+            chol_tile_dmma(stage + ba * bstride, stage + bb * bstride, i0, j0, c1, kk4, warp, lane, nwarps);
+            // release this tile's buffers the next tile does not use (no block
+            // barrier: warps run ahead until a fill they need has not landed)
+            __syncwarp();
+#pragma unroll
+            for (int b = 0; b < kStageBufs; ++b)
+                if ((b == ba || b == bb) && tag[b] != i1 && tag[b] != j1) {
+                    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(empty + b)) : "memory");
+                    rel[b] = 1, tag[b] = -1;
+                }
+        }
+        __syncthreads();
+        // fills still in flight (after a wait gave up) complete before the buffers go
+        int expired = 0;
+#pragma unroll
+        for (int b = 0; b < kStageBufs; ++b)
+            if (pend[b] && !bar_wait(full + b, par[b])) expired = 1;
+        expired = __syncthreads_or(expired);
+        if (threadIdx.x == 0) {
+            for (int b = 0; b < 2 * kStageBufs; ++b)
+                asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(full + b)) : "memory");
+            if (expired) ctl.brk = 2;
+        }
+        __syncthreads();
     }
 
     // chol_update for the plain form with 512 threads: a 4x4 micro-tile per
@@ -593,7 +796,7 @@ struct Block {
                     for (int u = 0; u < kB; ++u) {
                         const int e = e0 + u * blockDim.x, k = e / kCholTile, r = e % kCholTile;
                         const bool kin = e < tot && k < kk;
-                        const double* col = L + (int64_t)(k0 + k) * n;
+                        const double* col = L + (int64_t)(k0 + k) * ldl;
                         va[u] = (kin && i0 + r < n) ? col[i0 + r] : 0.0;
                         v0[u] = (kin && j0 + r < c1) ? col[j0 + r] : 0.0;
                         v1[u] = (two && kin && j1 + r < c1) ? col[j1 + r] : 0.0;
@@ -642,7 +845,7 @@ struct Block {
             if (seg < na) col = k0 + seg, row = min(i0 + r, n - 1);
             else if (seg < na + nb) col = k0 + seg - na, row = min(j0 + r, c1 - 1);
             else col = j0 + seg - na - nb, row = min(i0 + r, n - 1);
-            asm volatile("prefetch.L2 [%0];" ::"l"(L + (int64_t)col * n + row));
+            asm volatile("prefetch.L2 [%0];" ::"l"(L + (int64_t)col * ldl + row));
         }
     }
 
@@ -655,7 +858,7 @@ struct Block {
         double* D11 = stage;  // D11[c * kk + r] = L(kb + r, kb + c), r >= c
         for (int e = threadIdx.x; e < kk * kk; e += blockDim.x) {
             const int r = e % kk, c = e / kk;
-            D11[e] = r >= c ? L[(int64_t)(kb + c) * n + kb + r] : 0.0;
+            D11[e] = r >= c ? L[(int64_t)(kb + c) * ldl + kb + r] : 0.0;
         }
         __syncthreads();
         for (int k = 0; k < kk; ++k) {
@@ -676,13 +879,13 @@ struct Block {
         }
         for (int e = threadIdx.x; e < kk * kk; e += blockDim.x) {
             const int r = e % kk, c = e / kk;
-            if (r >= c) L[(int64_t)(kb + c) * n + kb + r] = D11[e];
+            if (r >= c) L[(int64_t)(kb + c) * ldl + kb + r] = D11[e];
         }
         // rows below the block, one per thread
         for (int i = ke + threadIdx.x; i < n; i += blockDim.x) {
             double a[kCholMaxPanel];
 #pragma unroll
-            for (int k = 0; k < kCholMaxPanel; ++k) a[k] = k < kk ? L[(int64_t)(kb + k) * n + i] : 0.0;
+            for (int k = 0; k < kCholMaxPanel; ++k) a[k] = k < kk ? L[(int64_t)(kb + k) * ldl + i] : 0.0;
 #pragma unroll
             for (int j = 0; j < kCholMaxPanel; ++j) {
                 if (j < kk) {
@@ -694,7 +897,7 @@ struct Block {
             }
 #pragma unroll
             for (int k = 0; k < kCholMaxPanel; ++k)
-                if (k < kk) L[(int64_t)(kb + k) * n + i] = a[k];
+                if (k < kk) L[(int64_t)(kb + k) * ldl + i] = a[k];
         }
         __syncthreads();
         return true;
@@ -719,7 +922,7 @@ struct Block {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     const int i = i0 + r0 + u, j = j0 + c0 + v;
-                    c[u][v] = (i < n && j < jend && i >= j) ? L[(int64_t)j * n + i] : 0.0;
+                    c[u][v] = (i < n && j < jend && i >= j) ? L[(int64_t)j * ldl + i] : 0.0;
                 }
             for (int k = 0; k < kk; ++k) {
                 const double2 a01 = *reinterpret_cast<const double2*>(As + k * TS + r0);
@@ -737,7 +940,7 @@ struct Block {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
                     const int i = i0 + r0 + u, j = j0 + c0 + v;
-                    if (i < n && j < jend && i >= j) L[(int64_t)j * n + i] = c[u][v];
+                    if (i < n && j < jend && i >= j) L[(int64_t)j * ldl + i] = c[u][v];
                 }
         }
     }
@@ -766,26 +969,35 @@ struct Block {
             const int tc = tcs + 8 * u;
             const bool act = !(i0 + tr + 7 < j0 + tc);
             const int i = i0 + tr + g, ja = j0 + tc + 2 * q, jb = ja + 1;
-            c[u][0] = (act && i < n && ja < jend && i >= ja) ? L[(int64_t)ja * n + i] : 0.0;
-            c[u][1] = (act && i < n && jb < jend && i >= jb) ? L[(int64_t)jb * n + i] : 0.0;
+            c[u][0] = (act && i < n && ja < jend && i >= ja) ? L[(int64_t)ja * ldl + i] : 0.0;
+            c[u][1] = (act && i < n && jb < jend && i >= jb) ? L[(int64_t)jb * ldl + i] : 0.0;
         }
     }
 
     __device__ void chol_tile_dmma(const double* As, const double* Bs, int i0, int j0, int jend, int kk4, int warp,
                                    int lane, int nwarps) {
-        double* L = Lt;
-        const int g = lane >> 2, q = lane & 3;
         for (int s = warp; s < kStrips; s += nwarps) {
             const int tr = (s % 8) * 8, tcs = (s / 8) * 32;
             if (i0 + tr + 7 < j0 + tcs) continue;  // the whole strip above the diagonal (warp-uniform)
             double c[4][2];
             dmma_load_c(s, i0, j0, jend, lane, c);
+            dmma_strip<4>(s, c, As, Bs, i0, j0, jend, kk4, lane);
+        }
+    }
+
+    // Strip s of the tile at (i0, j0): C (loaded into c) -= A B over kk4 staged
+    // k rows, stored back. kDmmaChains accumulation chains per fragment (k
+    // steps rotate over c and cx, summed at the end) cut the dependent-DMMA
+    // wait; the mixed form's tolerance admits the reassociation.
+    template <int kDmmaChains>
+    __device__ void dmma_strip(int s, double (&c)[4][2], const double* As, const double* Bs, int i0, int j0, int jend,
+                               int kk4, int lane) {
+        double* L = Lt;
+        const int g = lane >> 2, q = lane & 3;
+        const int tr = (s % 8) * 8, tcs = (s / 8) * 32;
+        {
             // blocks u < nact are active: the columns grow with u (warp-uniform)
             const int d = i0 + tr + 7 - j0 - tcs, nact = d >= 24 ? 4 : d / 8 + 1;
-            // kDmmaChains accumulation chains per fragment (k steps rotate over
-            // c and cx, summed at the end) cut the dependent-DMMA wait; the
-            // mixed form's tolerance admits the reassociation.
-            constexpr int kDmmaChains = 4;
             double cx[kDmmaChains - 1][4][2];
 #pragma unroll
             for (int h = 0; h < kDmmaChains - 1; ++h)
@@ -828,8 +1040,8 @@ struct Block {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = i0 + tr + g, ja = j0 + tcs + 8 * u + 2 * q, jb = ja + 1;
-                if (u < nact && i < n && ja < jend && i >= ja) L[(int64_t)ja * n + i] = c[u][0];
-                if (u < nact && i < n && jb < jend && i >= jb) L[(int64_t)jb * n + i] = c[u][1];
+                if (u < nact && i < n && ja < jend && i >= ja) L[(int64_t)ja * ldl + i] = c[u][0];
+                if (u < nact && i < n && jb < jend && i >= jb) L[(int64_t)jb * ldl + i] = c[u][1];
             }
         }
     }
@@ -838,7 +1050,7 @@ struct Block {
     __device__ void lower_matvec(const double* x, double* y) {
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             double s = 0.0;
-            for (int j = 0; j <= i; ++j) s += Lt[(int64_t)j * n + i] * x[j];
+            for (int j = 0; j <= i; ++j) s += Lt[(int64_t)j * ldl + i] * x[j];
             y[i] = s;
         }
     }
@@ -1256,6 +1468,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
         const int N = ch.N, n = 3 * N;
         B.N = N;
         B.n = n;
+        B.ldl = chol_ld(n);
         B.hi = ch.hstar > 0.0;
         if constexpr (!kMixed) {
             B.D = a.d_in_smem ? (sm + lay.D) : (scr + scl.D);
@@ -1357,7 +1570,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 } else {
                     if (ch.hi_method == BDCU_HI_CHOLESKY) {
                         // dense FP64 D straight into the factor's storage (lower part)
-                        B.build_rpy(R, B.Lt, n);
+                        B.build_rpy(R, B.Lt, B.ldl);
                     }
                 }
             }
@@ -1376,7 +1589,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 if constexpr (!kMixed) ok = B.cholesky(B.D, B.ldd, false);
                 else ok = B.cholesky(nullptr, 0, true);
                 if (!ok) {
-                    if (tid == 0) ctl.status |= BDCU_ST_NOT_PD;
+                    if (tid == 0) ctl.status |= ctl.brk == 2 ? BDCU_ST_TIMEOUT : BDCU_ST_NOT_PD;
                     __syncthreads();
                     break;
                 }
@@ -1405,11 +1618,11 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                     if constexpr (!kMixed) {
                         ok = B.cholesky(B.D, B.ldd, false);
                     } else {
-                        B.build_rpy(R, B.Lt, n);
+                        B.build_rpy(R, B.Lt, B.ldl);
                         ok = B.cholesky(nullptr, 0, true);
                     }
                     if (!ok) {
-                        if (tid == 0) ctl.status |= BDCU_ST_NOT_PD;
+                        if (tid == 0) ctl.status |= ctl.brk == 2 ? BDCU_ST_TIMEOUT : BDCU_ST_NOT_PD;
                         __syncthreads();
                         break;
                     }
@@ -1585,7 +1798,7 @@ __global__ void __launch_bounds__(512, 1) integrate_kernel(const RunArgs a) {
                 // D (and a factor made this step) are dead until the next
                 // step rebuilds them: drop their L2 lines unwritten
                 if (B.hi && !a.d_in_smem) discard_l2(B.D, (int64_t)n * B.ldd);
-                if (chol_used) discard_l2(B.Lt, (int64_t)n * n);
+                if (chol_used) discard_l2(B.Lt, (int64_t)n * B.ldl);
                 __syncthreads();
             }
         }

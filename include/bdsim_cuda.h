@@ -95,10 +95,14 @@ enum {
                                   stopped (the reference aborts,
                                   src/numerics.hpp:31-36,72) */
     BDCU_ST_NONFINITE = 16,    /* positions became NaN/Inf; chain stopped */
-    BDCU_ST_BAD_PARAM = 32     /* WLCbounded sigma>1 or ExactSqrt; chain
+    BDCU_ST_BAD_PARAM = 32,    /* WLCbounded sigma>1 or ExactSqrt; chain
                                   stopped (reference aborts) */
+    BDCU_ST_TIMEOUT = 64       /* a bounded wait inside the kernel (the
+                                  blocked Cholesky's tile copies) gave up;
+                                  chain stopped (no counterpart) */
 };
-#define BDCU_ST_FATAL_MASK (BDCU_ST_NOT_PD | BDCU_ST_RTSAFE_FAIL | BDCU_ST_NONFINITE | BDCU_ST_BAD_PARAM)
+#define BDCU_ST_FATAL_MASK \
+    (BDCU_ST_NOT_PD | BDCU_ST_RTSAFE_FAIL | BDCU_ST_NONFINITE | BDCU_ST_BAD_PARAM | BDCU_ST_TIMEOUT)
 
 /* ---- error codes returned by entry points ---- */
 enum {
