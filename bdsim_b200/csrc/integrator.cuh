@@ -626,9 +626,11 @@ struct Block {
     }
 
     // Wait for phase `parity` of bar; false if the bounded wait expired.
+    // (at most ~1 s of the global timer, and at most 2^24 polls)
     __device__ static bool bar_wait(uint64_t* bar, uint32_t parity) {
         const uint32_t mb = smem_addr(bar);
-        for (int it = 0; it < (1 << 20); ++it) {
+        uint64_t t0 = 0;
+        for (int it = 0; it < (1 << 24); ++it) {
             uint32_t done;
             asm volatile(
                 "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -636,6 +638,11 @@ struct Block {
                 : "r"(mb), "r"(parity)
                 : "memory");
             if (done) return true;
+            if ((it & 255) == 0) {
+                const uint64_t now = global_ns();
+                if (it == 0) t0 = now;
+                else if (now - t0 > 1000000000ull) return false;
+            }
         }
         return false;
     }

@@ -15,8 +15,8 @@
 // Host code sees only a stand-in for the array's name; its device address is
 // taken once per device with cudaGetSymbolAddress (the first call on a device
 // does it, and the first call after the device's context was replaced, e.g.
-// by cudaDeviceReset; make that first call before any stream capture on the
-// device).
+// by cudaDeviceReset). The entry point cannot be captured in a graph: it
+// stages its records and tables from pageable host vectors freed on return.
 // Every call shares the array and it keeps the last call's contents: the work
 // counters are cleared on each call, and everything else is written before it
 // is read. Calls that overlap on the GPU (two streams, two host threads) race

@@ -385,8 +385,11 @@ int bdcu_check_chains(int n_chains, const bdcu_phys* phys, const bdcu_sim* sim, 
      blocks as fit (fewer than bdcu_run may use).
    - The first call on a device takes the array's device address
      (cudaGetSymbolAddress), and so does the first call after the device's
-     context was replaced (cudaDeviceReset): make that call before any stream
-     capture on that device.
+     context was replaced (cudaDeviceReset).
+   - It must not be called inside stream capture: each call copies its
+     records, work list and tables from pageable host buffers that are freed
+     when it returns (the copies finish before it returns; a captured graph
+     would replay freed host memory).
    - Every call shares the array and leaves its contents behind; the work
      counters are cleared by each call. Calls that overlap on the GPU race on the
      array: serialise them. */
