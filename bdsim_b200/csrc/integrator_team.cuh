@@ -387,7 +387,7 @@ struct TeamChain {
         // pair (d = 0, s clamped to 1e-24) takes the near branch with om1 = 1
         // exactly in FP32 and om2 d = 0: it contributes the identity block.
         bool one_slot = false;
-        if constexpr (T > 1 && Q == 2) one_slot = __all_sync(kFull, !valid(1));
+        if constexpr (Q == 2) one_slot = __all_sync(kFull, !valid(1));
         const int nq = one_slot ? 1 : Q;
         if constexpr (K == 1) {
             // the Lanczos, Chebyshev, upsilon and corrector products: partner
