@@ -141,7 +141,7 @@ __device__ __forceinline__ void matvec_dense_k(const double* __restrict__ D, int
 #pragma unroll
         for (int r = 0; r < K; ++r) s[r] = 0.0;
         const double* col = D + i;
-#pragma unroll 4
+#pragma unroll 8
         for (int j = 0; j < n; ++j) {
             const double d = col[(int64_t)j * ld];
 #pragma unroll
@@ -173,7 +173,7 @@ __device__ __forceinline__ void matvec_dense(const double* __restrict__ D, int l
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double s = 0.0;
         const double* col = D + i;
-#pragma unroll 8
+#pragma unroll 16  // (16 loads of D in flight per row: +4.5% on the plain form over 8; 32 was slower)
         for (int j = 0; j < n; ++j) s += col[(int64_t)j * ld] * x[j];
         y[i] = s;
     }
