@@ -381,9 +381,9 @@ struct TeamChain {
         // In units of h*: with d = (R_j - R_b)/h*, s = |d|^2, rho = s^-1/2,
         //   far  (s >= 4 pi): om1 = rho (K1 + K2 rho^2), om2 = rho^3 (K1 - K3 rho^2)
         //   near (s <  4 pi): om1 = 1 - C3 s rho,         om2 = C7 rho
-        // and y_b += om1 x_j + om2 (d.x_j) d, with the branch folded into
-        // selected factors, om1 = B U + A and om2 = P V (selects run on the
-        // integer pipe, the FP32 pipe does one FFMA and one FMUL). The self
+        // and y_b += om1 x_j + om2 (d.x_j) d; the single products compute
+        // both branches' weights and select each once, the fused ones fold
+        // the branch into selected factors, om1 = B U + A, om2 = P V. The self
         // pair (d = 0, s clamped to 1e-24) takes the near branch with om1 = 1
         // exactly in FP32 and om2 d = 0: it contributes the identity block.
         bool one_slot = false;
@@ -402,6 +402,7 @@ struct TeamChain {
                     a[q][d] = make_float2(0.f, 0.f);
                 }
             const float2 k1 = make_float2(K1, K1), k2 = make_float2(K2, K2), mk3 = make_float2(-K3, -K3);
+            const float2 mc3 = make_float2(-C3, -C3), c7 = make_float2(C7, C7), one = make_float2(1.f, 1.f);
             const int n2 = (N + 1) & ~1;
             // not unrolled: this loop is inlined at every product's call site
 #pragma unroll 1
@@ -425,11 +426,13 @@ struct TeamChain {
                         const float2 u = __ffma2_rn(k2, t, k1), v = __ffma2_rn(mk3, t, k1);
                         const float2 r = __fmul2_rn(sq, rho), rt = __fmul2_rn(rho, t);
                         const bool fx = sq.x >= 12.566370614359172f, fy = sq.y >= 12.566370614359172f;
-                        const float2 om1 = __ffma2_rn(make_float2(fx ? rho.x : -C3, fy ? rho.y : -C3),
-                                                      make_float2(fx ? u.x : r.x, fy ? u.y : r.y),
-                                                      make_float2(fx ? 0.f : 1.f, fy ? 0.f : 1.f));
-                        const float2 om2 = __fmul2_rn(make_float2(fx ? rt.x : C7, fy ? rt.y : C7),
-                                                      make_float2(fx ? v.x : rho.x, fy ? v.y : rho.y));
+                        // both branches' weights, then one select each (a far
+                        // weight of the clamped self pair may be infinite: it
+                        // is not selected)
+                        const float2 f1 = __fmul2_rn(rho, u), f2 = __fmul2_rn(rt, v);
+                        const float2 n1 = __ffma2_rn(mc3, r, one), n2 = __fmul2_rn(c7, rho);
+                        const float2 om1 = make_float2(fx ? f1.x : n1.x, fy ? f1.y : n1.y);
+                        const float2 om2 = make_float2(fx ? f2.x : n2.x, fy ? f2.y : n2.y);
                         const float2 tt =
                             __fmul2_rn(om2, __ffma2_rn(dz, xj[2], __ffma2_rn(dy, xj[1], __fmul2_rn(dx, xj[0]))));
                         a[q][0] = __ffma2_rn(tt, dx, __ffma2_rn(om1, xj[0], a[q][0]));
