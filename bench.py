@@ -206,10 +206,11 @@ def compare_observables(m, p):
     return out
 
 
-def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
+def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form, team_shape=None):
     """Through the host-buffer entry point: pinned R/RNG in, integrate one
     chunk (a cold spectral cache per call, as a reference integrate call),
-    R/RNG/status out -- every step."""
+    R/RNG/status out -- every step. team_shape: (warps, beads per thread) of
+    the N=50 bucket, as the device-resident leg's autotuner chose it."""
     from bdsim_b200 import _abi
     from bdsim_b200.engine import Context, form_code
     n = len(Rs)
@@ -220,6 +221,8 @@ def run_e2e(torch, Rs, phys, sim, steps, warmup, seed0, form):
     s.time_start = 0.0
     s.time_end = (CHUNK - 1) * DT
     ctx.set_chains([phys] * n, [s] * n, [N_BEADS] * n)
+    if team_shape is not None:
+        ctx.set_team_shape(0, *team_shape)
     R = torch.from_numpy(np.concatenate(Rs)).pin_memory()
     rng = torch.tensor([(1, -1, seed0 + i) for i in range(n)], dtype=torch.int32).pin_memory()
     status = torch.zeros(n, dtype=torch.int32).pin_memory()
@@ -491,7 +494,12 @@ def main():
         barrier()
         r["total_ms"] = reduce_max(sum(r["ms"]), dist, device="cuda")
         results["mixed_k4"] = r
-    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, max(3, args.steps // 2), max(3, args.warmup), first, "mixed")
+    # (the same chunks of the same chains as the device-resident leg: a step's
+    # cost depends on how far the chains have relaxed)
+    # and the team shape the device leg ran with
+    e2e_shape = next((sh for sh in results.get("mixed", {}).get("shape", []) if len(sh) == 2), None)
+    e2e = None if args.no_e2e else run_e2e(torch, Rs, phys, sim, args.steps, max(3, args.warmup), first, "mixed",
+                                           team_shape=e2e_shape)
     serving = light = None
     if args.serving_seconds > 0 and set(forms) == {"plain", "mixed"}:
         # the serving configuration as stated (overload), then a lighter stream
