@@ -95,22 +95,57 @@ cudaError_t launch_forces(const DevChain* chains, int n_chains, int n_max, const
 // = Kramers stress tau_ij = sum_mu (R_mu - R_c)_i F_mu,j. One warp per chain,
 // sums over beads in a warp butterfly (not the host's order: last-bit
 // differences from numpy).
-__global__ void observables_kernel(const DevChain* __restrict__ chains, int n_chains, const double* __restrict__ R,
-                                   const double* __restrict__ F, double* __restrict__ out) {
+// One warp per chain, every chain's warp launched at once (no loop over
+// chains), so the loads of all chains are in flight together. A chain of up to
+// 64 beads is read once into registers (two beads per lane, R and F issued
+// together); longer chains take a second pass over R. Each lane sums its beads
+// in order, then the lanes' sums are reduced by shuffles: the same arithmetic
+// either way.
+__global__ void __launch_bounds__(256) observables_kernel(const DevChain* __restrict__ chains, int n_chains,
+                                                          const double* __restrict__ R, const double* __restrict__ F,
+                                                          double* __restrict__ out) {
     const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_chains; c += nw) {
-        const int N = chains[c].N;
-        const double* r = R + 3 * chains[c].bead_off;
-        const double* f = F + 3 * chains[c].bead_off;
-        double s[10];
+    const int c = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (c >= n_chains) return;
+    const int N = chains[c].N;
+    const double* r = R + 3 * chains[c].bead_off;
+    const double* f = F + 3 * chains[c].bead_off;
+    double s[10];
+    const double inv = N > 0 ? 1.0 / N : 0.0;
+    if (N <= 64) {
+        double rr[2][3], ff[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int m = lane + 32 * q;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                rr[q][d] = m < N ? r[3 * m + d] : 0.0;
+                ff[q][d] = m < N ? f[3 * m + d] : 0.0;
+            }
+        }
+        for (int d = 0; d < 3; ++d) s[d] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (lane + 32 * q < N)
+                for (int d = 0; d < 3; ++d) s[d] += rr[q][d];
+        for (int d = 0; d < 3; ++d)
+            for (int o = 16; o > 0; o >>= 1) s[d] += __shfl_xor_sync(0xffffffffu, s[d], o);
+        const double cx = s[0] * inv, cy = s[1] * inv, cz = s[2] * inv;
+        for (int k = 0; k < 10; ++k) s[k] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (lane + 32 * q < N) {
+                const double x[3] = {rr[q][0] - cx, rr[q][1] - cy, rr[q][2] - cz};
+                s[0] += x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) s[1 + 3 * i + j] += x[i] * ff[q][j];
+            }
+    } else {
         for (int d = 0; d < 3; ++d) s[d] = 0.0;
         for (int m = lane; m < N; m += 32)
             for (int d = 0; d < 3; ++d) s[d] += r[3 * m + d];
-        for (int d = 0; d < 3; ++d) {
+        for (int d = 0; d < 3; ++d)
             for (int o = 16; o > 0; o >>= 1) s[d] += __shfl_xor_sync(0xffffffffu, s[d], o);
-        }
-        const double inv = N > 0 ? 1.0 / N : 0.0;
         const double cx = s[0] * inv, cy = s[1] * inv, cz = s[2] * inv;
         for (int k = 0; k < 10; ++k) s[k] = 0.0;
         for (int m = lane; m < N; m += 32) {
@@ -119,19 +154,19 @@ __global__ void observables_kernel(const DevChain* __restrict__ chains, int n_ch
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) s[1 + 3 * i + j] += x[i] * f[3 * m + j];
         }
-        for (int k = 0; k < 10; ++k)
-            for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
-        if (lane == 0) {
-            out[10 * (int64_t)c] = s[0] * inv;
-            for (int k = 1; k < 10; ++k) out[10 * (int64_t)c + k] = s[k];
-        }
+    }
+    for (int k = 0; k < 10; ++k)
+        for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+    if (lane == 0) {
+        out[10 * (int64_t)c] = s[0] * inv;
+        for (int k = 1; k < 10; ++k) out[10 * (int64_t)c + k] = s[k];
     }
 }
 
 cudaError_t launch_observables(const DevChain* chains, int n_chains, const double* R, const double* F, double* out,
                                cudaStream_t s) {
-    const int warps = n_chains < 148 * 64 ? n_chains : 148 * 64;
-    observables_kernel<<<(warps + 7) / 8, 256, 0, s>>>(chains, n_chains, R, F, out);
+    if (n_chains < 1) return cudaSuccess;
+    observables_kernel<<<(unsigned)(((int64_t)n_chains + 7) / 8), 256, 0, s>>>(chains, n_chains, R, F, out);
     return cudaGetLastError();
 }
 
