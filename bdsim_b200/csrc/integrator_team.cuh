@@ -389,17 +389,18 @@ struct TeamChain {
         bool one_slot = false;
         if constexpr (Q == 2) one_slot = __all_sync(kFull, !valid(1));
         const int nq = one_slot ? 1 : Q;
-        if constexpr (K == 1) {
-            // the Lanczos, Chebyshev, upsilon and corrector products: partner
-            // beads two at a time in packed FP32x2
-            float2 nb[Q][3], a[Q][3];
+        {
+            // every product (the Lanczos, Chebyshev, upsilon and corrector
+            // ones, and the fused sets of K = 2, 3): partner beads two at a
+            // time in packed FP32x2
+            float2 nb[Q][3], a[K][Q][3];
 #pragma unroll
             for (int q = 0; q < Q; ++q)
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const float v = valid(q) ? -S.ps[d][bead(q)] : 0.f;
                     nb[q][d] = make_float2(v, v);
-                    a[q][d] = make_float2(0.f, 0.f);
+                    for (int r = 0; r < K; ++r) a[r][q][d] = make_float2(0.f, 0.f);
                 }
             const float2 k1 = make_float2(K1, K1), k2 = make_float2(K2, K2), mk3 = make_float2(-K3, -K3);
             const float2 mc3 = make_float2(-C3, -C3), c7 = make_float2(C7, C7), one = make_float2(1.f, 1.f);
@@ -407,11 +408,11 @@ struct TeamChain {
             // not unrolled: this loop is inlined at every product's call site
 #pragma unroll 1
             for (int j = 0; j < n2; j += 2) {
-                float2 pj[3], xj[3];
+                float2 pj[3], xj[K][3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     pj[d] = *reinterpret_cast<const float2*>(&S.ps[d][j]);
-                    xj[d] = *reinterpret_cast<const float2*>(&S.xk[0][d][j]);
+                    for (int r = 0; r < K; ++r) xj[r][d] = *reinterpret_cast<const float2*>(&S.xk[r][d][j]);
                 }
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
@@ -433,55 +434,13 @@ struct TeamChain {
                         const float2 n1 = __ffma2_rn(mc3, r, one), n2 = __fmul2_rn(c7, rho);
                         const float2 om1 = make_float2(fx ? f1.x : n1.x, fy ? f1.y : n1.y);
                         const float2 om2 = make_float2(fx ? f2.x : n2.x, fy ? f2.y : n2.y);
-                        const float2 tt =
-                            __fmul2_rn(om2, __ffma2_rn(dz, xj[2], __ffma2_rn(dy, xj[1], __fmul2_rn(dx, xj[0]))));
-                        a[q][0] = __ffma2_rn(tt, dx, __ffma2_rn(om1, xj[0], a[q][0]));
-                        a[q][1] = __ffma2_rn(tt, dy, __ffma2_rn(om1, xj[1], a[q][1]));
-                        a[q][2] = __ffma2_rn(tt, dz, __ffma2_rn(om1, xj[2], a[q][2]));
-                    }
-                }
-            }
-            sync();
-#pragma unroll
-            for (int q = 0; q < Q; ++q)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) acc[0][q][d] = valid(q) ? a[q][d].x + a[q][d].y : 0.f;
-        } else {
-            // the fused products of a step (K = 2, 3), once or twice per
-            // step: scalar FP32, fewer live registers than the packed form
-            float pb[Q][3];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) pb[q][d] = valid(q) ? S.ps[d][bead(q)] : 0.f;
-#pragma unroll
-                for (int r = 0; r < K; ++r)
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
-            }
-#pragma unroll 1
-            for (int j = 0; j < N; ++j) {
-                const float px = S.ps[0][j], py = S.ps[1][j], pz = S.ps[2][j];
-                float xj[K][3];
-#pragma unroll
-                for (int r = 0; r < K; ++r)
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) xj[r][d] = S.xk[r][d][j];
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    if (q < nq) {
-                        const float dx = px - pb[q][0], dy = py - pb[q][1], dz = pz - pb[q][2];
-                        const float sq = fmaxf(dx * dx + dy * dy + dz * dz, 1e-24f);
-                        const float rho = rsqrtf(sq), t = rho * rho;
-                        const bool far = sq >= 12.566370614359172f;
-                        const float om1 = fmaf(far ? rho : -C3, far ? fmaf(K2, t, K1) : sq * rho, far ? 0.f : 1.f);
-                        const float om2 = (far ? rho * t : C7) * (far ? fmaf(-K3, t, K1) : rho);
 #pragma unroll
                         for (int r = 0; r < K; ++r) {
-                            const float tt = om2 * (dx * xj[r][0] + dy * xj[r][1] + dz * xj[r][2]);
-                            acc[r][q][0] += om1 * xj[r][0] + tt * dx;
-                            acc[r][q][1] += om1 * xj[r][1] + tt * dy;
-                            acc[r][q][2] += om1 * xj[r][2] + tt * dz;
+                            const float2 tt = __fmul2_rn(
+                                om2, __ffma2_rn(dz, xj[r][2], __ffma2_rn(dy, xj[r][1], __fmul2_rn(dx, xj[r][0]))));
+                            a[r][q][0] = __ffma2_rn(tt, dx, __ffma2_rn(om1, xj[r][0], a[r][q][0]));
+                            a[r][q][1] = __ffma2_rn(tt, dy, __ffma2_rn(om1, xj[r][1], a[r][q][1]));
+                            a[r][q][2] = __ffma2_rn(tt, dz, __ffma2_rn(om1, xj[r][2], a[r][q][2]));
                         }
                     }
                 }
@@ -489,11 +448,9 @@ struct TeamChain {
             sync();
 #pragma unroll
             for (int q = 0; q < Q; ++q)
-                if (!valid(q))
 #pragma unroll
-                    for (int r = 0; r < K; ++r)
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) acc[r][q][d] = 0.f;
+                for (int d = 0; d < 3; ++d)
+                    for (int r = 0; r < K; ++r) acc[r][q][d] = valid(q) ? a[r][q][d].x + a[r][q][d].y : 0.f;
         }
     }
 
