@@ -381,9 +381,8 @@ struct TeamChain {
         // In units of h*: with d = (R_j - R_b)/h*, s = |d|^2, rho = s^-1/2,
         //   far  (s >= 4 pi): om1 = rho (K1 + K2 rho^2), om2 = rho^3 (K1 - K3 rho^2)
         //   near (s <  4 pi): om1 = 1 - C3 s rho,         om2 = C7 rho
-        // and y_b += om1 x_j + om2 (d.x_j) d; the single products compute
-        // both branches' weights and select each once, the fused ones fold
-        // the branch into selected factors, om1 = B U + A, om2 = P V. The self
+        // and y_b += om1 x_j + om2 (d.x_j) d; both branches' weights are
+        // computed and each is selected once. The self
         // pair (d = 0, s clamped to 1e-24) takes the near branch with om1 = 1
         // exactly in FP32 and om2 d = 0: it contributes the identity block.
         bool one_slot = false;
