@@ -416,8 +416,8 @@ int build_plan(bdcu_ctx* ctx, int form) {
         Bucket b;
         b.id = id;
         b.kernel = id < kFirstBlockBucket ? BDCU_KERNEL_TEAM : BDCU_KERNEL_BLOCK;
-        b.team_warps = id < kFirstBlockBucket ? (1 << id) : 0;
-        b.team_q = id < kFirstBlockBucket ? 2 : 0;
+        b.team_warps = id < kFirstBlockBucket ? kDefaultTeamShape[id][0] : 0;
+        b.team_q = id < kFirstBlockBucket ? kDefaultTeamShape[id][1] : 0;
         b.count = (int)L.size();
         b.max_beads = ctx->chains_h[L.front()].N;
         b.min_beads = ctx->chains_h[L.back()].N;

@@ -143,7 +143,7 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
     std::vector<std::vector<int32_t>> lists(kMaxBuckets);
     for (int i = 0; i < n_chains; ++i) lists[bucket_of(recs[i], form)].push_back(i);
     struct Launch {
-        int id, team_warps, block, grid, v_cap, d_in_smem, n_max, need_d, need_lz, count;
+        int id, team_warps, team_q, block, grid, v_cap, d_in_smem, n_max, need_d, need_lz, count;
         size_t smem, per_block;
         int64_t stride, order_off;
     };
@@ -170,14 +170,15 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
         int per_sm = 0;
         if (id < kFirstBlockBucket) {
             any_team = true;
-            l.team_warps = 1 << id;
-            l.smem = (size_t)team_smem(l.team_warps, 2, l.n_max);
+            l.team_warps = kDefaultTeamShape[id][0];
+            l.team_q = kDefaultTeamShape[id][1];
+            l.smem = (size_t)team_smem(l.team_warps, l.team_q, l.n_max);
             if (l.smem > ctx->max_smem) return fail(ctx, BDCU_E_LIMIT, "bdcu_run_static: team kernel shared memory too large");
-            e = occupancy_mixed_team(l.team_warps, 2, l.smem, &per_sm);
+            e = occupancy_mixed_team(l.team_warps, l.team_q, l.smem, &per_sm);
             l.stride = l.need_d ? team_scratch_doubles(l.n_max) : 1;
-            l.per_block = sizeof(double) * (size_t)l.stride * teams_per_cta(l.team_warps, 2);
-            l.block = 32 * l.team_warps * teams_per_cta(l.team_warps, 2);
-            l.grid = (l.count + teams_per_cta(l.team_warps, 2) - 1) / teams_per_cta(l.team_warps, 2);
+            l.per_block = sizeof(double) * (size_t)l.stride * teams_per_cta(l.team_warps, l.team_q);
+            l.block = 32 * l.team_warps * teams_per_cta(l.team_warps, l.team_q);
+            l.grid = (l.count + teams_per_cta(l.team_warps, l.team_q) - 1) / teams_per_cta(l.team_warps, l.team_q);
         } else {
             std::vector<int> d_opts = (!mixed && l.need_d) ? std::vector<int>{1, 0} : std::vector<int>{0};
             std::vector<int> v_opts = l.need_lz ? std::vector<int>{kLanczosCold, kLanczosWarm, 0} : std::vector<int>{0};
@@ -293,7 +294,7 @@ extern "C" int bdcu_run_static(bdcu_ctx* ctx, int n_chains, const bdcu_phys* phy
         a.xs_pow = reinterpret_cast<const uint32_t*>(b + o_cols);
         a.a_pow = reinterpret_cast<const uint32_t*>(b + o_apow);
         if (l.id < kFirstBlockBucket)
-            e = launch_mixed_team(l.team_warps, 2, a, l.grid, l.smem, s);
+            e = launch_mixed_team(l.team_warps, l.team_q, a, l.grid, l.smem, s);
         else
             e = mixed ? launch_mixed(a, l.grid, l.block, l.smem, s) : launch_plain(a, l.grid, l.block, l.smem, s);
         if (e != cudaSuccess)

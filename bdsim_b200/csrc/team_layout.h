@@ -75,11 +75,18 @@ __host__ __device__ inline int64_t team_scratch_doubles(int n_max) {
     return (int64_t)kLanczosCold * round_up8(n_max) + (int64_t)n_max * n_max;
 }
 
-// Team width of the default shape (Q = 2) for a chain of N beads (0: beyond
-// the team kernel).
+// Team width with two beads per thread for a chain of N beads, which names
+// its team bucket (0: beyond the team kernel).
 __host__ __device__ inline int team_warps_for(int N) {
     return N <= 64 ? 1 : N <= 128 ? 2 : N <= 256 ? 4 : N <= 512 ? 8 : 0;
 }
+
+// The team shape (warps, beads per thread) of team buckets 0..3 (N <= 64,
+// 128, 256, 512) when none is tuned or pinned: one bead per thread on 2 and 4
+// warps up to N = 128 (at N = 50, (2,1) ran 7.30 M chain-steps/s against 6.5 M
+// for (1,2); at N = 100, (4,1) 1.78 M against 1.53 M for (2,2)), two beads per
+// thread above.
+constexpr int kDefaultTeamShape[4][2] = {{2, 1}, {4, 1}, {4, 2}, {8, 2}};
 
 // The team shapes compiled into the library: (warps, beads per thread).
 constexpr int kNumTeamShapes = 7;

@@ -276,8 +276,9 @@ int bdcu_ran1(bdcu_ctx* ctx, int n_chains, int32_t* rng, int n_per_chain, double
    each bucket as one persistent launch over a device work list ordered
    largest chain first; buckets run concurrently, forked from the context
    stream and joined back to it. In the FP32-mixed form a chain of N <= 512
-   beads (and no Cholesky method) runs on a team of 1, 2, 4 or 8 warps (N <=
-   64, 128, 256, 512; buckets 0..3); every other chain runs one chain per
+   beads (and no Cholesky method) runs on the team kernel in buckets 0..3 (N <=
+   64, 128, 256, 512), by default with (warps per chain, beads per thread) =
+   (2,1), (4,1), (4,2), (8,2) unless tuned or pinned; every other chain runs one chain per
    thread block, in buckets 4..7 split at N = 64, 128 and 256. Once a plan is
    built (first bdcu_run after a change of records, selection or form) a
    bdcu_run enqueues only a memset, event records/waits and kernel launches,

@@ -58,10 +58,10 @@ def test_plan_buckets_cover_the_batch(uneven):
     plan = ens.plan()
     assert sum(b["n_chains"] for b in plan) == len(NS)
     by_id = {b["bucket"]: b for b in plan}
-    # FP32-mixed: teams of 1, 2, 4, 8 warps per chain
-    for bid, (T, lo, hi) in enumerate([(1, 8, 64), (2, 65, 128), (4, 129, 256), (8, 257, 300)]):
+    # FP32-mixed default team shapes: (2,1), (4,1), (4,2), (8,2) warps x beads per thread
+    for bid, (T, Q, lo, hi) in enumerate([(2, 1, 8, 64), (4, 1, 65, 128), (4, 2, 129, 256), (8, 2, 257, 300)]):
         b = by_id[bid]
-        assert b["kernel"] == _abi.KERNEL_TEAM and b["team_warps"] == T, b
+        assert b["kernel"] == _abi.KERNEL_TEAM and (b["team_warps"], b["team_beads_per_thread"]) == (T, Q), b
         assert (b["min_beads"], b["max_beads"]) == (lo, hi), b
         assert b["n_chains"] == sum(lo <= n <= hi for n in NS)
     # the plain form runs every chain one per block
